@@ -1,0 +1,174 @@
+"""Test infrastructure only: ctypes access to the oracle.
+
+* ``Oracle``    -- the plain-C restatement (oracle/cellato_oracle.c, liboracle.so).
+* ``RefOracle`` -- the reference's own CPU code compiled by oracle/Makefile into
+  oracle/_ref/libcellato_ref.so (present where the reference tree was available
+  at build time; it travels with the repository snapshot).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use this
+module, and only as the checker or the timed CPU baseline.  Cells are uint8
+dictionary indices (the integer the bit planes encode).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libcellato_ref.so")
+
+RULES = ["game-of-life", "forest-fire", "wire", "excitable", "brian",
+         "maze", "cyclic", "fluid", "critters", "traffic"]
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u8p)
+
+
+class Oracle:
+    """The C restatement of the reference standard CPU path."""
+
+    def __init__(self, path: str = LIB_PATH):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle`")
+        lib = ctypes.CDLL(path)
+        lib.oracle_run.argtypes = [ctypes.c_int, _u8p, _u8p, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.oracle_pack.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p,
+                                    ctypes.c_int, ctypes.c_int, _u8p]
+        lib.oracle_unpack.argtypes = lib.oracle_pack.argtypes
+        lib.oracle_checksum.argtypes = [ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_uint64)]
+        lib.oracle_rule_name.restype = ctypes.c_char_p
+        lib.oracle_rule_from_name.argtypes = [ctypes.c_char_p]
+        self.lib = lib
+
+    def planes(self, rule: int) -> int:
+        return self.lib.oracle_planes(rule)
+
+    def states(self, rule: int) -> int:
+        return self.lib.oracle_states(rule)
+
+    def state_value(self, rule: int, index: int) -> int:
+        return self.lib.oracle_state_value(rule, index)
+
+    def run(self, rule: int, cells: np.ndarray, steps: int, t0: int = 0, threads: int = 0) -> np.ndarray:
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        out = np.empty_like(cells)
+        threads = threads or (os.cpu_count() or 1)
+        rc = self.lib.oracle_run(rule, _ptr(cells), _ptr(out), X, Y, t0, steps, threads)
+        if rc != 0:
+            raise RuntimeError(f"oracle_run failed: {rc}")
+        return out
+
+    def pack(self, layout: int, word_bits: int, nb: int, cells: np.ndarray) -> np.ndarray:
+        """Returns an array of shape (nb, X*Y/8) uint8: the planes as bytes."""
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        out = np.zeros((nb, X * Y // 8), dtype=np.uint8)
+        rc = self.lib.oracle_pack(layout, word_bits, nb, _ptr(cells), X, Y, _ptr(out))
+        if rc != 0:
+            raise ValueError(f"oracle_pack rejected layout={layout} W={word_bits} X={X} Y={Y}")
+        return out
+
+    def unpack(self, layout: int, word_bits: int, nb: int, planes: np.ndarray, X: int, Y: int) -> np.ndarray:
+        planes = np.ascontiguousarray(planes, dtype=np.uint8)
+        out = np.empty((Y, X), dtype=np.uint8)
+        rc = self.lib.oracle_unpack(layout, word_bits, nb, _ptr(planes), X, Y, _ptr(out))
+        if rc != 0:
+            raise ValueError("oracle_unpack rejected its arguments")
+        return out
+
+    def checksum(self, rule: int, cells: np.ndarray) -> str:
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        out = (ctypes.c_uint64 * 16)()
+        self.lib.oracle_checksum(rule, _ptr(cells), X, Y, out)
+        return "-".join(str(v) for v in out)
+
+
+class RefOracle:
+    """The reference's own CPU code (compiled from the reference tree)."""
+
+    def __init__(self, path: str = REF_PATH):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+        lib = ctypes.CDLL(path)
+        lib.cref_run_standard.argtypes = [ctypes.c_int, _u8p, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.cref_run_standard_mt.argtypes = [ctypes.c_int, _u8p, _u8p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int]
+        lib.cref_run_bit_planes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p, _u8p,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.cref_pack.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p, ctypes.c_int,
+                                  ctypes.c_int, _u8p]
+        lib.cref_pack.restype = ctypes.c_longlong
+        lib.cref_reference_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p]
+        lib.cref_checksum.argtypes = [ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                      ctypes.c_int]
+        lib.cref_rule_name.restype = ctypes.c_char_p
+        self.lib = lib
+
+    def name(self, rule: int) -> str:
+        return self.lib.cref_rule_name(rule).decode()
+
+    def planes(self, rule: int) -> int:
+        return self.lib.cref_needed_bits(rule)
+
+    def states(self, rule: int) -> int:
+        return self.lib.cref_number_of_states(rule)
+
+    def state_value(self, rule: int, index: int) -> int:
+        return self.lib.cref_state_value(rule, index)
+
+    def run_standard(self, rule: int, cells: np.ndarray, steps: int, threads: int = 1) -> np.ndarray:
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        out = np.empty_like(cells)
+        if threads == 1:
+            rc = self.lib.cref_run_standard(rule, _ptr(cells), _ptr(out), X, Y, steps)
+        else:
+            rc = self.lib.cref_run_standard_mt(rule, _ptr(cells), _ptr(out), X, Y, steps, threads)
+        if rc != 0:
+            raise RuntimeError(f"reference standard run failed: {rc}")
+        return out
+
+    def run_bit_planes(self, rule: int, word_bits: int, tiled: bool, cells: np.ndarray, steps: int) -> np.ndarray:
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        out = np.empty_like(cells)
+        rc = self.lib.cref_run_bit_planes(rule, word_bits, int(tiled), _ptr(cells), _ptr(out), X, Y, steps)
+        if rc != 0:
+            raise RuntimeError(f"reference bit-plane run failed: {rc}")
+        return out
+
+    def pack(self, rule: int, word_bits: int, tiled: bool, cells: np.ndarray) -> np.ndarray:
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        nb = self.planes(rule)
+        out = np.zeros((nb, X * Y // 8), dtype=np.uint8)
+        r = self.lib.cref_pack(rule, word_bits, int(tiled), _ptr(cells), X, Y, _ptr(out))
+        if r < 0:
+            raise RuntimeError("reference pack failed")
+        return out
+
+    def reference_init(self, rule: int, X: int, Y: int, seed: int) -> np.ndarray:
+        out = np.empty((Y, X), dtype=np.uint8)
+        rc = self.lib.cref_reference_init(rule, X, Y, seed, _ptr(out))
+        if rc != 0:
+            raise RuntimeError("reference init failed")
+        return out
+
+    def checksum(self, rule: int, cells: np.ndarray) -> str:
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        buf = ctypes.create_string_buffer(1024)
+        n = self.lib.cref_checksum(rule, _ptr(cells), X, Y, buf, 1024)
+        if n < 0:
+            raise RuntimeError("reference checksum failed")
+        return buf.value.decode()
