@@ -1,0 +1,31 @@
+#ifndef CYCLIC_CONFIG_HPP
+#define CYCLIC_CONFIG_HPP
+
+#include "../common_init.hpp"
+#include "./algorithm.hpp"
+#include "memory/state_dictionary.hpp"
+
+namespace cyclic {
+
+struct config {
+    static constexpr char name[] = "cyclic";
+    static constexpr double average_halo_radius = 1.0;
+    using algorithm = cyclic_algorithm;
+    using cell_state = cyclic_cell_state;
+    using state_dictionary = cellato::memory::grids::int_based_state_dictionary<BITS>;
+
+    struct input {
+        // uniform over the 32 states; the grid utility's default seed (12345)
+        struct random {
+            static std::vector<cell_state> init(cellato::run::run_params& params) {
+                std::vector<std::tuple<cell_state, double>> d;
+                for (int s = 0; s < STATES; ++s) d.emplace_back(s, 1.0 / STATES);
+                return cellato::automata::iid_grid<cell_state>(params, d, 12345);
+            }
+        };
+    };
+};
+
+}  // namespace cyclic
+
+#endif

@@ -1,0 +1,114 @@
+"""ctypes binding of the C ABI in include/cellato_b200.h.
+
+The shared library is built in-tree (``make -C 2026-cellato-smpt-journal_b200``)
+into ``lib/libcellato_b200.so``.  There is no fallback: if the library is
+missing, ``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libcellato_b200.so")
+
+OK, EINVAL, EINVAL_DIMS, ESMEM, ECUDA, ETIMEDOUT, ENOMEM, EUNSUPPORTED = range(8)
+STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "EINVAL_DIMS", 3: "ESMEM", 4: "ECUDA", 5: "ETIMEDOUT",
+                6: "ENOMEM", 7: "EUNSUPPORTED"}
+
+LAYOUT_BIT_PLANES = 0
+LAYOUT_TILED_BIT_PLANES = 1
+LAYOUTS = {"bit_planes": LAYOUT_BIT_PLANES, "tiled_bit_planes": LAYOUT_TILED_BIT_PLANES}
+
+# Every symbol include/cellato_b200.h declares (checked by the CPU tests).
+EXPORTED = [
+    "cellato_version", "cellato_last_error", "cellato_rule_from_name", "cellato_rule_name",
+    "cellato_rule_planes", "cellato_rule_states", "cellato_plane_bytes", "cellato_check_dims",
+    "cellato_planes_alloc", "cellato_planes_free", "cellato_planes_upload", "cellato_planes_download",
+    "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
+]
+
+
+class CellatoError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_PP = ctypes.POINTER(ctypes.c_void_p)
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built; run `make -C {PKG_DIR}`")
+    lib = ctypes.CDLL(path)
+    lib.cellato_version.restype = ctypes.c_char_p
+    lib.cellato_last_error.restype = ctypes.c_char_p
+    lib.cellato_rule_from_name.argtypes = [ctypes.c_char_p]
+    lib.cellato_rule_name.restype = ctypes.c_char_p
+    lib.cellato_plane_bytes.restype = ctypes.c_size_t
+    lib.cellato_plane_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.cellato_planes_alloc.argtypes = [ctypes.c_int, ctypes.c_size_t, _PP]
+    lib.cellato_planes_free.argtypes = [ctypes.c_int, _PP]
+    lib.cellato_planes_upload.argtypes = [ctypes.c_int, _PP, _PP, ctypes.c_size_t, _vp]
+    lib.cellato_planes_download.argtypes = [ctypes.c_int, _PP, _PP, ctypes.c_size_t, _vp]
+    i = ctypes.c_int
+    lib.cellato_run_simple.argtypes = [i, i, i, _PP, _PP, i, i, i, i, _vp, ctypes.POINTER(i)]
+    lib.cellato_run_temporal.argtypes = [i, i, i, _PP, _PP, i, i, i, i, i, i, _vp, ctypes.POINTER(i)]
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != OK:
+        raise CellatoError(status, load().cellato_last_error().decode())
+
+
+def ptr_array(ptrs) -> ctypes.Array:
+    arr = (ctypes.c_void_p * max(1, len(ptrs)))()
+    for i, p in enumerate(ptrs):
+        arr[i] = p
+    return arr
+
+
+def rule_id(name_or_id) -> int:
+    if isinstance(name_or_id, int):
+        return name_or_id
+    r = load().cellato_rule_from_name(name_or_id.encode())
+    if r < 0:
+        raise ValueError(f"unknown automaton {name_or_id!r}")
+    return r
+
+
+def rule_planes(rule) -> int:
+    return load().cellato_rule_planes(rule_id(rule))
+
+
+def rule_states(rule) -> int:
+    return load().cellato_rule_states(rule_id(rule))
+
+
+def rule_name(rule) -> str:
+    return load().cellato_rule_name(rule_id(rule)).decode()
+
+
+def run_simple(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,
+               stream: int = 0) -> int:
+    """Returns 1 when the result ended in planes_b, else 0."""
+    out = ctypes.c_int(0)
+    check(load().cellato_run_simple(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),
+                                    X, Y, t0, steps, stream, ctypes.byref(out)))
+    return out.value
+
+
+def run_temporal(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,
+                 k: int, tile_rows: int = 0, stream: int = 0) -> int:
+    out = ctypes.c_int(0)
+    check(load().cellato_run_temporal(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),
+                                      X, Y, t0, steps, k, tile_rows, stream, ctypes.byref(out)))
+    return out.value

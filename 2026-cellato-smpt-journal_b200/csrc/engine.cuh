@@ -1,0 +1,494 @@
+// B200 kernels for the bit-plane hot path: a streaming single-step kernel
+// (the "simple" traverser) and a temporally blocked shared-memory kernel (the
+// "temporal" traverser), both driving one lowered rule (b200/lower.cuh).
+//
+// Internal representation: linear rows of 32-bit plane words (bit i of word w
+// of row y = cell (32w + i, y)).  The byte formats the caller owns are adapted
+// at load/store:
+//   LAYOUT_LINEAR  bit_planes (reference include/memory/bit_planes_grid.hpp:255-263).
+//                  32- and 64-bit words are the same bytes (little endian), so
+//                  one kernel serves both word sizes.
+//   LAYOUT_TILED4  tiled_bit_planes with 32-bit words: 8 x 4 cell tiles, bit
+//                  y_bit*8 + x_bit (tiled_bit_planes_grid.hpp:270-282).
+//   LAYOUT_TILED8  tiled_bit_planes with 64-bit words: 8 x 8 cell tiles.
+// A linear word spans 4 horizontally adjacent tiles; byte r of a tile word is
+// row r of the tile, so tiles <-> linear rows is a 4x4 byte transpose per group
+// of four 32-bit tile rows (8 PRMTs), done in registers.
+#ifndef CELLATO_B200_ENGINE_CUH
+#define CELLATO_B200_ENGINE_CUH
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "b200/lower.cuh"
+
+namespace cellato::b200 {
+
+enum : int { LAYOUT_LINEAR = 0, LAYOUT_TILED4 = 1, LAYOUT_TILED8 = 2 };
+
+constexpr int MAX_PLANES = 8;
+
+struct plane_set {
+    word* p[MAX_PLANES];
+};
+
+// Rows per tile word (band height) of a layout.
+template <int LAYOUT>
+constexpr int band_rows() {
+    return LAYOUT == LAYOUT_TILED4 ? 4 : (LAYOUT == LAYOUT_TILED8 ? 8 : 1);
+}
+
+// ------------------------------------------------------------ byte transpose
+// (t0, t1, t2, t3): four 32-bit words, byte r of t_j = row r of column-block j.
+// Returns row-major: r_r = (t0.b_r, t1.b_r, t2.b_r, t3.b_r).  Self-inverse.
+__device__ __forceinline__ void transpose4x4(word& a, word& b, word& c, word& d) {
+    const word u = __byte_perm(a, b, 0x5140);  // a0 b0 a1 b1
+    const word v = __byte_perm(a, b, 0x7362);  // a2 b2 a3 b3
+    const word w = __byte_perm(c, d, 0x5140);  // c0 d0 c1 d1
+    const word x = __byte_perm(c, d, 0x7362);  // c2 d2 c3 d3
+    a = __byte_perm(u, w, 0x5410);             // a0 b0 c0 d0
+    b = __byte_perm(u, w, 0x7632);             // a1 b1 c1 d1
+    c = __byte_perm(v, x, 0x5410);             // a2 b2 c2 d2
+    d = __byte_perm(v, x, 0x7632);             // a3 b3 c3 d3
+}
+
+// Load the R rows of linear word gx of band b (tile row b) of one plane.
+//   linear: R == 1, word gx of row b.
+//   tiled : tiles 4gx .. 4gx+3 of tile row b, transposed to R row words.
+template <int LAYOUT>
+__device__ __forceinline__ void load_word_rows(const word* __restrict__ plane, int Xw, int b, int gx,
+                                               word (&rows)[band_rows<LAYOUT>()]) {
+    if constexpr (LAYOUT == LAYOUT_LINEAR) {
+        rows[0] = __ldg(plane + (size_t)b * Xw + gx);
+    } else if constexpr (LAYOUT == LAYOUT_TILED4) {
+        // 4 tiles x 4 bytes = one 16-byte vector
+        const uint4 t = __ldg(reinterpret_cast<const uint4*>(plane + ((size_t)b * Xw + gx) * 4));
+        word a = t.x, bb = t.y, c = t.z, d = t.w;
+        transpose4x4(a, bb, c, d);
+        rows[0] = a, rows[1] = bb, rows[2] = c, rows[3] = d;
+    } else {
+        // 4 tiles x 8 bytes: (lo, hi) per tile; lo = rows 0-3, hi = rows 4-7
+        const uint4* src = reinterpret_cast<const uint4*>(plane + ((size_t)b * Xw + gx) * 8);
+        const uint4 t01 = __ldg(src), t23 = __ldg(src + 1);
+        word l0 = t01.x, l1 = t01.z, l2 = t23.x, l3 = t23.z;
+        word h0 = t01.y, h1 = t01.w, h2 = t23.y, h3 = t23.w;
+        transpose4x4(l0, l1, l2, l3);
+        transpose4x4(h0, h1, h2, h3);
+        rows[0] = l0, rows[1] = l1, rows[2] = l2, rows[3] = l3;
+        rows[4] = h0, rows[5] = h1, rows[6] = h2, rows[7] = h3;
+    }
+}
+
+template <int LAYOUT>
+__device__ __forceinline__ void store_word_rows(word* __restrict__ plane, int Xw, int b, int gx,
+                                                const word (&rows)[band_rows<LAYOUT>()]) {
+    if constexpr (LAYOUT == LAYOUT_LINEAR) {
+        plane[(size_t)b * Xw + gx] = rows[0];
+    } else if constexpr (LAYOUT == LAYOUT_TILED4) {
+        word a = rows[0], bb = rows[1], c = rows[2], d = rows[3];
+        transpose4x4(a, bb, c, d);
+        *reinterpret_cast<uint4*>(plane + ((size_t)b * Xw + gx) * 4) = make_uint4(a, bb, c, d);
+    } else {
+        word l0 = rows[0], l1 = rows[1], l2 = rows[2], l3 = rows[3];
+        word h0 = rows[4], h1 = rows[5], h2 = rows[6], h3 = rows[7];
+        transpose4x4(l0, l1, l2, l3);
+        transpose4x4(h0, h1, h2, h3);
+        uint4* dst = reinterpret_cast<uint4*>(plane + ((size_t)b * Xw + gx) * 8);
+        dst[0] = make_uint4(l0, h0, l1, h1);
+        dst[1] = make_uint4(l2, h2, l3, h3);
+    }
+}
+
+// A lane's V consecutive words (gx a multiple of V, Xw a multiple of V) of the
+// R rows of band b; linear rows use one 8- or 16-byte vector access.
+template <int LAYOUT, int V>
+__device__ __forceinline__ void load_lane(const word* __restrict__ plane, int Xw, int b, int gx,
+                                          word (&rows)[band_rows<LAYOUT>()][V]) {
+    if constexpr (LAYOUT == LAYOUT_LINEAR && V == 4) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(plane + (size_t)b * Xw + gx));
+        rows[0][0] = q.x, rows[0][1] = q.y, rows[0][2] = q.z, rows[0][3] = q.w;
+    } else if constexpr (LAYOUT == LAYOUT_LINEAR && V == 2) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2*>(plane + (size_t)b * Xw + gx));
+        rows[0][0] = q.x, rows[0][1] = q.y;
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            word t[band_rows<LAYOUT>()];
+            load_word_rows<LAYOUT>(plane, Xw, b, gx + v, t);
+#pragma unroll
+            for (int r = 0; r < band_rows<LAYOUT>(); ++r) rows[r][v] = t[r];
+        }
+    }
+}
+
+template <int LAYOUT, int V>
+__device__ __forceinline__ void store_lane(word* __restrict__ plane, int Xw, int b, int gx,
+                                           const word (&rows)[band_rows<LAYOUT>()][V]) {
+    if constexpr (LAYOUT == LAYOUT_LINEAR && V == 4) {
+        *reinterpret_cast<uint4*>(plane + (size_t)b * Xw + gx) = make_uint4(rows[0][0], rows[0][1], rows[0][2], rows[0][3]);
+    } else if constexpr (LAYOUT == LAYOUT_LINEAR && V == 2) {
+        *reinterpret_cast<uint2*>(plane + (size_t)b * Xw + gx) = make_uint2(rows[0][0], rows[0][1]);
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            word t[band_rows<LAYOUT>()];
+#pragma unroll
+            for (int r = 0; r < band_rows<LAYOUT>(); ++r) t[r] = rows[r][v];
+            store_word_rows<LAYOUT>(plane, Xw, b, gx + v, t);
+        }
+    }
+}
+
+// ------------------------------------------------------------- lane helpers
+// Words to the left / right of a lane's V words, from the neighbouring lanes
+// (lane 0 and lane 31 receive the wrapped value of lane 31 / lane 0, which is
+// correct when the warp spans the whole row and is overridden otherwise).
+__device__ __forceinline__ word from_left_lane(word v) {
+    return __shfl_sync(0xffffffffu, v, (threadIdx.x + 31) & 31);
+}
+__device__ __forceinline__ word from_right_lane(word v) {
+    return __shfl_sync(0xffffffffu, v, (threadIdx.x + 1) & 31);
+}
+
+template <class Net, int V>
+struct row_window {
+    using feat = typename Net::feat;
+    feat f[V];
+};
+
+// Features of one row from its raw words: C[p][v] plus left/right edge words.
+template <class Net, int NB, int V>
+__device__ __forceinline__ void build_feat(const word (&C)[NB][V], const word (&L)[NB], const word (&R)[NB],
+                                           typename Net::feat (&out)[V]) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        word c[NB], l[NB], r[NB];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            c[p] = C[p][v];
+            l[p] = v == 0 ? L[p] : C[p][v == 0 ? 0 : v - 1];
+            r[p] = v == V - 1 ? R[p] : C[p][v == V - 1 ? 0 : v + 1];
+        }
+        out[v] = Net::make_feat(c, l, r);
+    }
+}
+
+// ======================================================= single-step kernel
+// One launch = one time step.  Each warp owns a horizontal segment of 32*V
+// words (lane l: words seg*32V + l*V .. +V-1) and walks down the CTA's rows in
+// bands of R rows with a rolling window of three rows' features; every input
+// word is loaded once per CTA row range (+2 halo rows), every output word
+// stored once.
+template <class Net, int NB, int LAYOUT, int V, int TP, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, plane_set out, int Xw, int Yb,
+                                                                 int Y, int bands_per_cta) {
+    constexpr int R = band_rows<LAYOUT>();
+    using feat = typename Net::feat;
+    const int lane = threadIdx.x & 31;
+    const int seg = blockIdx.x * WARPS + (threadIdx.x >> 5);
+    const int gx_raw = seg * 32 * V + lane * V;          // first word of this lane (unwrapped)
+    const bool owns = gx_raw < Xw;                        // lanes past the row end only feed neighbours
+    const int gx = gx_raw % Xw;
+    const int gx_left = (seg * 32 * V + Xw - 1) % Xw;     // word left of the segment
+    const int gx_right = (seg * 32 * V + 32 * V) % Xw;    // word right of the segment
+    const bool seg_spans_row = (32 * V == Xw);  // lane 0 / 31 neighbours are lanes 31 / 0
+
+    const int b0 = blockIdx.y * bands_per_cta;
+    const int b1 = min(Yb, b0 + bands_per_cta);
+    if (b0 >= b1) return;
+
+    auto load_band = [&](int b, word (&raw)[R][NB][V], word (&L)[R][NB], word (&Rr)[R][NB]) {
+        const int bw = (b % Yb + Yb) % Yb;
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            word rows[R][V];
+            load_lane<LAYOUT, V>(in.p[p], Xw, bw, gx, rows);
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+#pragma unroll
+                for (int v = 0; v < V; ++v) raw[r][p][v] = rows[r][v];
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+                L[r][p] = from_left_lane(raw[r][p][V - 1]);
+                Rr[r][p] = from_right_lane(raw[r][p][0]);
+            }
+        if (!seg_spans_row && (lane == 0 || lane == 31)) {
+            const int gxe = lane == 0 ? gx_left : gx_right;
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+                word rows[R];
+                load_word_rows<LAYOUT>(in.p[p], Xw, bw, gxe, rows);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (lane == 0)
+                        L[r][p] = rows[r];
+                    else
+                        Rr[r][p] = rows[r];
+                }
+            }
+        }
+    };
+
+    word cur[R][NB][V], curL[R][NB], curR[R][NB];
+    word nxt[R][NB][V], nxtL[R][NB], nxtR[R][NB];
+    feat up[V], mid[V], dn[V];
+
+    // row above the first band: last row of the previous band
+    load_band(b0 - 1, nxt, nxtL, nxtR);
+    {
+        word C[NB][V], Lw[NB], Rw[NB];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) C[p][v] = nxt[R - 1][p][v];
+            Lw[p] = nxtL[R - 1][p];
+            Rw[p] = nxtR[R - 1][p];
+        }
+        build_feat<Net, NB, V>(C, Lw, Rw, up);
+    }
+    load_band(b0, cur, curL, curR);
+    {
+        word C[NB][V], Lw[NB], Rw[NB];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) C[p][v] = cur[0][p][v];
+            Lw[p] = curL[0][p];
+            Rw[p] = curR[0][p];
+        }
+        build_feat<Net, NB, V>(C, Lw, Rw, mid);
+    }
+
+    for (int b = b0; b < b1; ++b) {
+        load_band(b + 1, nxt, nxtL, nxtR);
+        word res[R][NB][V];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            word C[NB][V], Lw[NB], Rw[NB];
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) C[p][v] = r + 1 < R ? cur[r + 1 < R ? r + 1 : 0][p][v] : nxt[0][p][v];
+                Lw[p] = r + 1 < R ? curL[r + 1 < R ? r + 1 : 0][p] : nxtL[0][p];
+                Rw[p] = r + 1 < R ? curR[r + 1 < R ? r + 1 : 0][p] : nxtR[0][p];
+            }
+            build_feat<Net, NB, V>(C, Lw, Rw, dn);
+            const int y = b * R + r;
+            const int ypar = (y < Y ? y : y - Y) & 1;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                word o[NB];
+                Net::template eval<TP>(up[v], mid[v], dn[v], ypar, o);
+#pragma unroll
+                for (int p = 0; p < NB; ++p) res[r][p][v] = o[p];
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                up[v] = mid[v];
+                mid[v] = dn[v];
+            }
+        }
+        if (owns) {
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+                word rows[R][V];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int v = 0; v < V; ++v) rows[r][v] = res[r][p][v];
+                store_lane<LAYOUT, V>(out.p[p], Xw, b, gx, rows);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) cur[r][p][v] = nxt[r][p][v];
+                curL[r][p] = nxtL[r][p];
+                curR[r][p] = nxtR[r][p];
+            }
+    }
+}
+
+// ==================================================== temporal-blocked kernel
+// One launch = k time steps on a shared-memory tile of TH rows x 32V words
+// (one warp spans the tile width; lane l owns words l*V .. l*V+V-1 of every
+// row).  The tile carries a 1-word (32-cell) halo left and right and HY rows
+// above and below (HY >= k, a multiple of the band height), so after k steps
+// its interior -- words 1 .. 32V-2, rows HY .. TH-HY-1 -- is exact.
+//
+// Steps update the tile in place.  Warps own horizontal bands of the tile
+// (TH / WARPS rows each) and sweep them top-down: the rolling window keeps the
+// old value of the row above in registers, the row below is read before it is
+// overwritten, and horizontal neighbours come from lane shuffles of registers,
+// so no lane ever reads a word another lane writes within a step.  Only the
+// two rows bordering a band belong to other warps: they are read before the
+// first barrier of the step and every write happens after it.  At step t only
+// rows t .. TH-1-t are computed (the valid region shrinks by one row per step).
+template <class Net, int NB, int LAYOUT, int V, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plane_set out, int Xw, int Y, int t0,
+                                                              int k, int TH, int HY) {
+    constexpr int R = band_rows<LAYOUT>();
+    constexpr int TW = 32 * V;  // tile width in words
+    using feat = typename Net::feat;
+    extern __shared__ __align__(16) word tile[];  // [NB][TH][TW]
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int effW = TW - 2;
+    const int effH = TH - 2 * HY;
+    const int x0 = blockIdx.x * effW;  // first output word
+    const int y0 = blockIdx.y * effH;  // first output row
+    const int Yb = Y / R;
+
+    auto at = [&](int p, int r, int s) -> word& { return tile[((size_t)p * TH + r) * TW + s]; };
+
+    // ---- load the tile (rows wrap on the torus; words wrap per word)
+    for (int band = warp; band < TH / R; band += WARPS) {
+        const int gy0 = y0 - HY + band * R;                   // first global row of this band (unwrapped)
+        const int bw = ((gy0 / R) % Yb + Yb) % Yb;            // gy0 is a multiple of R
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int s = lane * V + v;
+            const int gx = ((x0 - 1 + s) % Xw + Xw) % Xw;
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+                word rows[R];
+                load_word_rows<LAYOUT>(in.p[p], Xw, bw, gx, rows);
+#pragma unroll
+                for (int r = 0; r < R; ++r) at(p, band * R + r, s) = rows[r];
+            }
+        }
+    }
+    __syncthreads();
+
+    const int rows_per_warp = TH / WARPS;
+    const int rw0 = warp * rows_per_warp;
+    const int rw1 = rw0 + rows_per_warp;
+
+    auto read_row = [&](int r, word (&C)[NB][V], word (&L)[NB], word (&Rr)[NB]) {
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            if constexpr (V % 4 == 0) {
+#pragma unroll
+                for (int v = 0; v < V; v += 4) {
+                    const uint4 q = *reinterpret_cast<const uint4*>(&at(p, r, lane * V + v));
+                    C[p][v] = q.x, C[p][v + 1] = q.y, C[p][v + 2] = q.z, C[p][v + 3] = q.w;
+                }
+            } else if constexpr (V % 2 == 0) {
+#pragma unroll
+                for (int v = 0; v < V; v += 2) {
+                    const uint2 q = *reinterpret_cast<const uint2*>(&at(p, r, lane * V + v));
+                    C[p][v] = q.x, C[p][v + 1] = q.y;
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v) C[p][v] = at(p, r, lane * V + v);
+            }
+            L[p] = from_left_lane(C[p][V - 1]);
+            Rr[p] = from_right_lane(C[p][0]);
+            if (lane == 0) L[p] = 0;   // beyond the tile: its halo absorbs the error
+            if (lane == 31) Rr[p] = 0;
+        }
+    };
+
+    auto write_row = [&](int r, const word (&o)[NB][V]) {
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            if constexpr (V % 4 == 0) {
+#pragma unroll
+                for (int v = 0; v < V; v += 4)
+                    *reinterpret_cast<uint4*>(&at(p, r, lane * V + v)) =
+                        make_uint4(o[p][v], o[p][v + 1], o[p][v + 2], o[p][v + 3]);
+            } else if constexpr (V % 2 == 0) {
+#pragma unroll
+                for (int v = 0; v < V; v += 2)
+                    *reinterpret_cast<uint2*>(&at(p, r, lane * V + v)) = make_uint2(o[p][v], o[p][v + 1]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v) at(p, r, lane * V + v) = o[p][v];
+            }
+        }
+    };
+
+    auto step = [&](int t, auto tp_tag) {
+        constexpr int TP = decltype(tp_tag)::value;
+        const int lo = max(rw0, t);
+        const int hi = min(rw1, TH - t);
+        word topC[NB][V], topL[NB], topR[NB], botC[NB][V], botL[NB], botR[NB];
+        if (lo < hi) {
+            read_row(lo - 1, topC, topL, topR);
+            read_row(hi, botC, botL, botR);
+        }
+        __syncthreads();
+        if (lo < hi) {
+            feat up[V], mid[V], dn[V];
+            build_feat<Net, NB, V>(topC, topL, topR, up);
+            {
+                word C[NB][V], L[NB], Rr[NB];
+                read_row(lo, C, L, Rr);
+                build_feat<Net, NB, V>(C, L, Rr, mid);
+            }
+            for (int r = lo; r < hi; ++r) {
+                if (r + 1 < hi) {
+                    word C[NB][V], L[NB], Rr[NB];
+                    read_row(r + 1, C, L, Rr);
+                    build_feat<Net, NB, V>(C, L, Rr, dn);
+                } else {
+                    build_feat<Net, NB, V>(botC, botL, botR, dn);
+                }
+                const int gy = ((y0 - HY + r) % Y + Y) % Y;
+                word o[NB][V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    word ov[NB];
+                    Net::template eval<TP>(up[v], mid[v], dn[v], gy & 1, ov);
+#pragma unroll
+                    for (int p = 0; p < NB; ++p) o[p][v] = ov[p];
+                }
+                write_row(r, o);
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    up[v] = mid[v];
+                    mid[v] = dn[v];
+                }
+            }
+        }
+        __syncthreads();
+    };
+
+    for (int t = 1; t <= k; ++t) {
+        if (((t0 + t - 1) & 1) == 0)
+            step(t, std::integral_constant<int, 0>{});
+        else
+            step(t, std::integral_constant<int, 1>{});
+    }
+
+    // ---- store the interior
+    for (int band = HY / R + warp; band < (TH - HY) / R; band += WARPS) {
+        const int gy0 = y0 - HY + band * R;
+        if (gy0 >= Y) continue;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int s = lane * V + v;
+            const int gx = x0 - 1 + s;
+            if (s < 1 || s > TW - 2 || gx >= Xw) continue;
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+                word rows[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) rows[r] = at(p, band * R + r, s);
+                store_word_rows<LAYOUT>(out.p[p], Xw, gy0 / R, gx, rows);
+            }
+        }
+    }
+}
+
+}  // namespace cellato::b200
+
+#endif  // CELLATO_B200_ENGINE_CUH

@@ -1,0 +1,129 @@
+// Per-rule launchers: instantiate the engine kernels for one automaton config
+// and expose them through a rule_ops table (one table per rule, one .cu file
+// per rule so the ten rules compile in parallel).  This is the B200
+// counterpart of the reference's explicit instantiations
+// (src/_shared/cuda_instantiation_template.cuh:77-193): the rule stays a C++
+// type and is lowered at compile time; the C ABI selects it by id.
+#ifndef CELLATO_B200_RULE_KERNELS_CUH
+#define CELLATO_B200_RULE_KERNELS_CUH
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "engine.cuh"
+
+namespace cellato::b200 {
+
+struct rule_ops {
+    const char* name;
+    int planes;  // needed_bits
+    int states;  // number_of_values
+    // one time step t (its parity selects the instantiation)
+    cudaError_t (*simple)(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t,
+                          cudaStream_t s);
+    // k fused steps from t0 on a TH-row tile with an HY-row halo
+    cudaError_t (*temporal)(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
+                            int TH, int HY, cudaStream_t s);
+    int temporal_words_per_lane;  // V of the temporal tile (tile width 32*V words)
+    int temporal_warps;
+};
+
+// Words per lane of the single-step kernel: as wide as registers allow.  A row
+// of features costs about 3 words per plane plus 5 per count target per lane
+// word, and three rows plus three bands of raw words are live.
+template <class Net, int NB, int R>
+constexpr int simple_words_per_lane() {
+    constexpr int feat_words = 3 * NB + 5 * Net::targets::size;
+    constexpr int per_v = 3 * feat_words + 3 * R * NB;
+    return per_v * 4 <= 128 ? 4 : (per_v * 2 <= 128 ? 2 : 1);
+}
+
+template <class A>
+struct rule_kernels {
+    using dict = typename A::state_dictionary;
+    using net = rule_net<dict, typename A::algorithm>;
+    static constexpr int NB = dict::needed_bits;
+    static_assert(NB <= MAX_PLANES, "too many planes");
+    static constexpr int SIMPLE_WARPS = 4;
+    static constexpr int TEMPORAL_V = NB <= 3 ? 2 : 1;
+    static constexpr int TEMPORAL_WARPS = 8;
+
+    template <int LAYOUT, int V>
+    static cudaError_t simple_v(const plane_set& in, const plane_set& out, int Xw, int Y, int t, cudaStream_t s) {
+        constexpr int R = band_rows<LAYOUT>();
+        const int Yb = Y / R;
+        const int segments = (Xw + 32 * V - 1) / (32 * V);
+        const int cta_x = (segments + SIMPLE_WARPS - 1) / SIMPLE_WARPS;
+        // enough warps to cover 148 SMs x 32 resident warps, at most 64 rows per CTA
+        long long want = 148LL * 32;
+        int bands = (int)std::max(1LL, std::min<long long>(64 / R, (long long)segments * Yb / want));
+        bands = std::max(1, bands);
+        const int cta_y = (Yb + bands - 1) / bands;
+        const dim3 grid(cta_x, cta_y), block(SIMPLE_WARPS * 32);
+        if (t & 1)
+            simple_step_kernel<net, NB, LAYOUT, V, 1, SIMPLE_WARPS><<<grid, block, 0, s>>>(in, out, Xw, Yb, Y, bands);
+        else
+            simple_step_kernel<net, NB, LAYOUT, V, 0, SIMPLE_WARPS><<<grid, block, 0, s>>>(in, out, Xw, Yb, Y, bands);
+        return cudaGetLastError();
+    }
+
+    template <int LAYOUT>
+    static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t,
+                                     cudaStream_t s) {
+        constexpr int VMAX = simple_words_per_lane<net, NB, band_rows<LAYOUT>()>();
+        if constexpr (VMAX >= 4)
+            if (Xw % 4 == 0) return simple_v<LAYOUT, 4>(in, out, Xw, Y, t, s);
+        if constexpr (VMAX >= 2)
+            if (Xw % 2 == 0) return simple_v<LAYOUT, 2>(in, out, Xw, Y, t, s);
+        return simple_v<LAYOUT, 1>(in, out, Xw, Y, t, s);
+    }
+
+    static cudaError_t simple(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t,
+                              cudaStream_t s) {
+        switch (layout) {
+            case LAYOUT_LINEAR: return simple_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t, s);
+            case LAYOUT_TILED4: return simple_layout<LAYOUT_TILED4>(in, out, Xw, Y, t, s);
+            case LAYOUT_TILED8: return simple_layout<LAYOUT_TILED8>(in, out, Xw, Y, t, s);
+        }
+        return cudaErrorInvalidValue;
+    }
+
+    template <int LAYOUT>
+    static cudaError_t temporal_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
+                                       int TH, int HY, cudaStream_t s) {
+        constexpr int V = TEMPORAL_V;
+        auto kern = temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS>;
+        const size_t smem = (size_t)NB * TH * 32 * V * sizeof(word);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int effW = 32 * V - 2, effH = TH - 2 * HY;
+        const dim3 grid((Xw + effW - 1) / effW, (Y + effH - 1) / effH), block(TEMPORAL_WARPS * 32);
+        kern<<<grid, block, smem, s>>>(in, out, Xw, Y, t0, k, TH, HY);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t temporal(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
+                                int TH, int HY, cudaStream_t s) {
+        switch (layout) {
+            case LAYOUT_LINEAR: return temporal_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t0, k, TH, HY, s);
+            case LAYOUT_TILED4: return temporal_layout<LAYOUT_TILED4>(in, out, Xw, Y, t0, k, TH, HY, s);
+            case LAYOUT_TILED8: return temporal_layout<LAYOUT_TILED8>(in, out, Xw, Y, t0, k, TH, HY, s);
+        }
+        return cudaErrorInvalidValue;
+    }
+
+    static rule_ops ops() {
+        return rule_ops{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS};
+    }
+};
+
+}  // namespace cellato::b200
+
+#define CELLATO_DEFINE_RULE_OPS(ID, CONFIG)                        \
+    namespace cellato::b200 {                                      \
+    extern const rule_ops rule_ops_##ID;                           \
+    const rule_ops rule_ops_##ID = rule_kernels<CONFIG>::ops();    \
+    }
+
+#endif  // CELLATO_B200_RULE_KERNELS_CUH

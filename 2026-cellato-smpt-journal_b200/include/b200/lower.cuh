@@ -1,0 +1,771 @@
+// Compile-time lowering of a rule AST (core/ast.hpp) into a bitwise network
+// over 32-bit plane words.
+//
+// Representation.  A `word` holds one bit of 32 horizontally consecutive cells
+// of one row (bit i = cell x0 + i, x0 a multiple of 32, least significant bit
+// leftmost -- the order of the reference linear bit planes,
+// include/memory/bit_planes_grid.hpp:255-263).  A value is `planes<B>`: B words,
+// plane i holding bit i of the value of each of the 32 cells.  A condition is a
+// single word.  Widths are tracked at compile time with exactly the rules of
+// the reference bit-sliced integer (include/core/vector_int.hpp):
+//   * from_constant<c> has width highest_bit(c) + 2, or 1 for c == 0 (:752-776)
+//   * plus wraps at the wider operand's width (:227-286)
+//   * modulo by 2^n truncates to n planes (bit_planes.hpp:163-182)
+//   * comparisons zero-extend the narrower operand (:423-590)
+//   * bit_and_ zero-fills and bit_or_ keeps the wider operand's extra planes (:625-700)
+//   * if_then_else selects per cell with the condition mask (bit_planes.hpp:87-107)
+// so every rule computes, cell for cell, what the reference standard evaluator
+// computes (include/evaluators/standard.hpp).
+//
+// Neighbourhood access.  The engine hands the lowering three `row_feat`s (the
+// rows above, at and below the output row) that it builds once per row when the
+// row enters its rolling window: the row's planes shifted by dx = -1, 0, +1, and
+// for every count target S of the rule the predicate "cell == S" at the three
+// dx, with its full-adder (3 cells) and half-adder (2 cells) partial sums.  A
+// Moore count is then a 3-operand carry-save addition of per-row partial sums
+// (8 LOP3s) instead of the reference's chain of seven ripple adders.
+//
+// Only radius-1 neighbourhoods are supported (neighbor_at offsets in -1..1),
+// the same limit as the reference tiled evaluator
+// (include/evaluators/tiled_bit_planes.hpp:117, :202).
+#ifndef CELLATO_B200_LOWER_CUH
+#define CELLATO_B200_LOWER_CUH
+
+#include <cstdint>
+#include <type_traits>
+#include <utility>
+
+#include "../core/ast.hpp"
+
+#if defined(__CUDACC__)
+#define CB_HD __host__ __device__ __forceinline__
+#else
+#define CB_HD inline
+#endif
+
+namespace cellato::b200 {
+
+using word = std::uint32_t;
+
+// ---------------------------------------------------------------- bit vectors
+template <int B>
+struct planes {
+    static_assert(B >= 1, "a value has at least one plane");
+    static constexpr int width = B;
+    word p[B];
+};
+
+template <class T>
+struct is_planes : std::false_type {};
+template <int B>
+struct is_planes<planes<B>> : std::true_type {};
+
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int cmin(int a, int b) { return a < b ? a : b; }
+
+constexpr int highest_bit(long long v) {
+    int h = -1;
+    for (int i = 0; i < 62; ++i)
+        if ((v >> i) & 1) h = i;
+    return h;
+}
+
+// Width of a literal: highest set bit + 2 (one spare zero plane), 1 for zero.
+constexpr int const_width(long long v) { return v == 0 ? 1 : highest_bit(v) + 2; }
+
+constexpr int exact_log2(long long v) { return highest_bit(v); }
+
+template <long long V>
+CB_HD planes<const_width(V)> from_constant() {
+    static_assert(V >= 0, "negative literals are not representable as bit planes");
+    planes<const_width(V)> r;
+#pragma unroll
+    for (int i = 0; i < const_width(V); ++i) r.p[i] = ((V >> i) & 1) ? ~word(0) : word(0);
+    return r;
+}
+
+// A condition used as a value is a one-plane vector.
+CB_HD planes<1> as_planes(word w) { return planes<1>{{w}}; }
+template <int B>
+CB_HD planes<B> as_planes(planes<B> v) { return v; }
+
+template <int N, int B>
+CB_HD planes<N> resize(planes<B> a) {
+    planes<N> r;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.p[i] = i < B ? a.p[i < B ? i : 0] : word(0);
+    return r;
+}
+
+// Ripple-carry add modulo 2^max(A, B).
+template <int A, int B>
+CB_HD planes<cmax(A, B)> add(planes<A> a, planes<B> b) {
+    constexpr int M = cmax(A, B), m = cmin(A, B);
+    planes<M> r;
+    word carry = 0;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        if (i < m) {
+            const word x = a.p[i] ^ b.p[i];
+            r.p[i] = x ^ carry;
+            carry = (a.p[i] & b.p[i]) | (carry & x);
+        } else {
+            const word w = A > B ? a.p[i < A ? i : 0] : b.p[i < B ? i : 0];
+            r.p[i] = w ^ carry;
+            carry = carry & w;
+        }
+    }
+    return r;
+}
+
+template <int A, int B>
+CB_HD planes<cmax(A, B)> bor(planes<A> a, planes<B> b) {
+    constexpr int M = cmax(A, B);
+    planes<M> r;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        const word x = i < A ? a.p[i < A ? i : 0] : word(0);
+        const word y = i < B ? b.p[i < B ? i : 0] : word(0);
+        r.p[i] = x | y;
+    }
+    return r;
+}
+
+template <int A, int B>
+CB_HD planes<cmax(A, B)> band(planes<A> a, planes<B> b) {
+    constexpr int M = cmax(A, B);
+    planes<M> r;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        const word x = i < A ? a.p[i < A ? i : 0] : word(0);
+        const word y = i < B ? b.p[i < B ? i : 0] : word(0);
+        r.p[i] = x & y;
+    }
+    return r;
+}
+
+template <int B>
+CB_HD planes<B> mask(planes<B> a, word m) {
+#pragma unroll
+    for (int i = 0; i < B; ++i) a.p[i] &= m;
+    return a;
+}
+
+template <int A, int B>
+CB_HD word eq(planes<A> a, planes<B> b) {
+    word r = ~word(0);
+#pragma unroll
+    for (int i = 0; i < cmax(A, B); ++i) {
+        const word x = i < A ? a.p[i < A ? i : 0] : word(0);
+        const word y = i < B ? b.p[i < B ? i : 0] : word(0);
+        r &= ~(x ^ y);
+    }
+    return r;
+}
+
+template <int A, int B>
+CB_HD word ne(planes<A> a, planes<B> b) { return ~eq(a, b); }
+
+// Unsigned a > b, most significant plane first.
+template <int A, int B>
+CB_HD word gt(planes<A> a, planes<B> b) {
+    word result = 0, decided = 0;
+#pragma unroll
+    for (int i = cmax(A, B) - 1; i >= 0; --i) {
+        const word x = i < A ? a.p[i < A ? i : 0] : word(0);
+        const word y = i < B ? b.p[i < B ? i : 0] : word(0);
+        result |= ~decided & x & ~y;
+        decided |= x ^ y;
+    }
+    return result;
+}
+
+template <int A, int B>
+CB_HD word lt(planes<A> a, planes<B> b) { return gt(b, a); }
+
+// "all NB planes spell the constant S" -- equals_to<S> of a stored state.
+template <int S, int NB>
+CB_HD word eq_const(const word* p) {
+    word r = ~word(0);
+#pragma unroll
+    for (int i = 0; i < NB; ++i) r &= ((S >> i) & 1) ? p[i] : ~p[i];
+    return r;
+}
+
+// Full adder / half adder on words (each output is one LOP3).
+CB_HD word xor3(word a, word b, word c) { return a ^ b ^ c; }
+CB_HD word maj3(word a, word b, word c) { return (a & b) | (c & (a ^ b)); }
+
+// Funnel shifts that bring a neighbour word's edge bit in.
+// shl1(prev, cur): bit i = cur bit i-1, bit 0 = prev bit 31   (cell x-1)
+// shr1(cur, next): bit i = cur bit i+1, bit 31 = next bit 0   (cell x+1)
+CB_HD word shl1(word prev, word cur) {
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_l(prev, cur, 1);
+#else
+    return (cur << 1) | (prev >> 31);
+#endif
+}
+CB_HD word shr1(word cur, word next) {
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_r(cur, next, 1);
+#else
+    return (cur >> 1) | (next << 31);
+#endif
+}
+
+// ------------------------------------------------------- collecting targets
+// Dictionary indices S of every count_neighbors<state_constant<V>, ...> node.
+template <int... S>
+struct ilist {
+    static constexpr int size = sizeof...(S);
+};
+
+template <class A, class B>
+struct icat;
+template <int... A, int... B>
+struct icat<ilist<A...>, ilist<B...>> {
+    using type = ilist<A..., B...>;
+};
+
+template <class... Ls>
+struct icat_all {
+    using type = ilist<>;
+};
+template <class L, class... Ls>
+struct icat_all<L, Ls...> {
+    using type = typename icat<L, typename icat_all<Ls...>::type>::type;
+};
+
+template <class L, int S>
+struct icontains;
+template <int S, int... Xs>
+struct icontains<ilist<Xs...>, S> {
+    static constexpr bool value = ((Xs == S) || ...);
+};
+
+template <class L>
+struct idedup {
+    using type = ilist<>;
+};
+template <int X, int... Xs>
+struct idedup<ilist<X, Xs...>> {
+    using rest = typename idedup<ilist<Xs...>>::type;
+    using type = std::conditional_t<icontains<rest, X>::value, rest, typename icat<ilist<X>, rest>::type>;
+};
+
+template <class L, int S>
+struct iindex;
+template <int S, int X, int... Xs>
+struct iindex<ilist<X, Xs...>, S> {
+    static constexpr int value = (X == S) ? 0 : 1 + iindex<ilist<Xs...>, S>::value;
+};
+template <int S>
+struct iindex<ilist<>, S> {
+    static constexpr int value = 0;
+};
+
+namespace ast = cellato::ast;
+
+template <class Dict, class E>
+struct count_targets {
+    using type = ilist<>;
+};
+
+template <class Dict, class N>
+struct count_targets_nb {
+    using type = ilist<>;
+};
+
+template <class Dict, auto V, class N>
+struct count_targets<Dict, ast::count_neighbors<ast::state_constant<V>, N>> {
+    using type = ilist<Dict::state_to_index(V)>;
+};
+template <class Dict, class T, class N>
+struct count_targets<Dict, ast::count_neighbors<T, N>> {
+    using type = typename count_targets<Dict, T>::type;
+};
+template <class Dict, class C, class T, class E>
+struct count_targets<Dict, ast::if_then_else<C, T, E>> {
+    using type = typename icat_all<typename count_targets<Dict, C>::type, typename count_targets<Dict, T>::type,
+                                   typename count_targets<Dict, E>::type>::type;
+};
+template <class Dict, class V>
+struct count_targets<Dict, ast::not_<V>> {
+    using type = typename count_targets<Dict, V>::type;
+};
+template <class Dict, class V, int b>
+struct count_targets<Dict, ast::has_bit_set<V, b>> {
+    using type = typename count_targets<Dict, V>::type;
+};
+template <class Dict, class... As>
+struct count_targets<Dict, ast::alternate_algorithms<As...>> {
+    using type = typename icat_all<typename count_targets<Dict, As>::type...>::type;
+};
+#define CB_BINARY_TARGETS(NODE)                                                                             \
+    template <class Dict, class L, class R>                                                                 \
+    struct count_targets<Dict, ast::NODE<L, R>> {                                                           \
+        using type =                                                                                        \
+            typename icat<typename count_targets<Dict, L>::type, typename count_targets<Dict, R>::type>::type; \
+    };
+CB_BINARY_TARGETS(and_)
+CB_BINARY_TARGETS(or_)
+CB_BINARY_TARGETS(bit_and_)
+CB_BINARY_TARGETS(bit_or_)
+CB_BINARY_TARGETS(plus)
+CB_BINARY_TARGETS(modulo)
+CB_BINARY_TARGETS(equals)
+CB_BINARY_TARGETS(not_equals)
+CB_BINARY_TARGETS(greater_than)
+CB_BINARY_TARGETS(less_than)
+#undef CB_BINARY_TARGETS
+
+template <class Dict, class E>
+using targets_of = typename idedup<typename count_targets<Dict, E>::type>::type;
+
+// ------------------------------------------------------------ per-row cache
+// Predicate "cell == S" at dx = -1, 0, +1 and its partial sums.
+struct count_cache {
+    word P[3];   // P[dx + 1]
+    word s3, c3; // P[0] + P[1] + P[2]  (sum, carry)
+    word s2, c2; // P[0] + P[2]
+};
+
+template <int NB, class Targets>
+struct row_feat {
+    word sh[3][NB];  // sh[dx + 1][plane]
+    count_cache cc[Targets::size > 0 ? Targets::size : 1];
+};
+
+// Builds a row's features from its own word (C), the word to its left (L) and
+// the word to its right (R), all NB planes.  Only bit 31 of L and bit 0 of R
+// matter.
+template <int NB, class Targets, int... S>
+CB_HD row_feat<NB, Targets> make_row_feat_impl(const word* C, const word* L, const word* R, ilist<S...>) {
+    row_feat<NB, Targets> f;
+#pragma unroll
+    for (int p = 0; p < NB; ++p) {
+        f.sh[0][p] = shl1(L[p], C[p]);
+        f.sh[1][p] = C[p];
+        f.sh[2][p] = shr1(C[p], R[p]);
+    }
+    int k = 0;
+    (
+        [&] {
+            // predicate first, shift second: one predicate per word instead of three
+            const word pc = eq_const<S, NB>(C);
+            const word pl = eq_const<S, NB>(L);
+            const word pr = eq_const<S, NB>(R);
+            count_cache& c = f.cc[k++];
+            c.P[0] = shl1(pl, pc);
+            c.P[1] = pc;
+            c.P[2] = shr1(pc, pr);
+            c.s3 = xor3(c.P[0], c.P[1], c.P[2]);
+            c.c3 = maj3(c.P[0], c.P[1], c.P[2]);
+            c.s2 = c.P[0] ^ c.P[2];
+            c.c2 = c.P[0] & c.P[2];
+        }(),
+        ...);
+    (void)k;
+    return f;
+}
+
+template <int NB, class Targets>
+CB_HD row_feat<NB, Targets> make_row_feat(const word* C, const word* L, const word* R) {
+    return make_row_feat_impl<NB, Targets>(C, L, R, Targets{});
+}
+
+// Evaluation context of one output word.  TP is the parity of the time step
+// (a compile-time constant: the engines instantiate both), ypar the parity of
+// the output row's global y.
+template <class RF, int TP>
+struct ctx {
+    const RF& up;
+    const RF& mid;
+    const RF& dn;
+    int ypar;
+
+    template <int dy>
+    CB_HD const RF& row() const {
+        if constexpr (dy < 0)
+            return up;
+        else if constexpr (dy > 0)
+            return dn;
+        else
+            return mid;
+    }
+    // Row holding the vertical Margolus partner: y+1 when (y + t) is even,
+    // y-1 otherwise (include/evaluators/standard.hpp:183-197).
+    CB_HD const RF& margolus_row() const { return ((ypar ^ TP) == 0) ? dn : up; }
+};
+
+// Bits whose horizontal Margolus partner is x+1: even x on even steps, odd x
+// on odd steps.  Word origins are multiples of 32, so x parity = bit parity.
+template <int TP>
+CB_HD constexpr word margolus_right_mask() { return TP == 0 ? word(0x55555555u) : word(0xAAAAAAAAu); }
+
+// --------------------------------------------------------------- the nodes
+template <class Dict, class Targets, class E>
+struct lower {
+    static_assert(sizeof(E) == 0, "AST node not supported by the B200 lowering");
+};
+
+// Evaluate node E (free function, so that node bodies can recurse by name).
+template <class Dict, class Targets, class E, class C>
+CB_HD auto ev(const C& c) {
+    return lower<Dict, Targets, E>::eval(c);
+}
+
+template <class T>
+CB_HD word as_cond(T v) {
+    if constexpr (std::is_same_v<T, word>)
+        return v;
+    else {
+        static_assert(std::is_same_v<T, planes<1>>, "a condition must be a single plane");
+        return v.p[0];
+    }
+}
+
+template <class Dict, class Targets, auto V>
+struct lower<Dict, Targets, ast::constant<V>> {
+    template <class C>
+    CB_HD static auto eval(const C&) { return from_constant<(long long)V>(); }
+};
+
+template <class Dict, class Targets, auto V>
+struct lower<Dict, Targets, ast::state_constant<V>> {
+    template <class C>
+    CB_HD static auto eval(const C&) { return from_constant<(long long)Dict::state_to_index(V)>(); }
+};
+
+template <class Dict, class Targets, int dx, int dy>
+struct lower<Dict, Targets, ast::neighbor_at<dx, dy>> {
+    static_assert(dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1, "neighbor_at offsets are limited to -1..1");
+    static constexpr int NB = Dict::needed_bits;
+    template <class C>
+    CB_HD static planes<NB> eval(const C& c) {
+        planes<NB> r;
+        const auto& row = c.template row<dy>();
+#pragma unroll
+        for (int p = 0; p < NB; ++p) r.p[p] = row.sh[dx + 1][p];
+        return r;
+    }
+};
+
+template <class Dict, class Targets, class Cn, class T, class E>
+struct lower<Dict, Targets, ast::if_then_else<Cn, T, E>> {
+    template <class C>
+    CB_HD static auto eval(const C& c) {
+        const word m = as_cond(ev<Dict, Targets, Cn>(c));
+        auto t = ev<Dict, Targets, T>(c);
+        auto e = ev<Dict, Targets, E>(c);
+        if constexpr (std::is_same_v<decltype(t), word> && std::is_same_v<decltype(e), word>)
+            return word((t & m) | (e & ~m));
+        else
+            return bor(mask(as_planes(t), m), mask(as_planes(e), ~m));
+    }
+};
+
+template <class Dict, class Targets, class L, class R>
+struct lower<Dict, Targets, ast::and_<L, R>> {
+    template <class C>
+    CB_HD static word eval(const C& c) {
+        return as_cond(ev<Dict, Targets, L>(c)) & as_cond(ev<Dict, Targets, R>(c));
+    }
+};
+
+template <class Dict, class Targets, class L, class R>
+struct lower<Dict, Targets, ast::or_<L, R>> {
+    template <class C>
+    CB_HD static word eval(const C& c) {
+        return as_cond(ev<Dict, Targets, L>(c)) | as_cond(ev<Dict, Targets, R>(c));
+    }
+};
+
+template <class Dict, class Targets, class V>
+struct lower<Dict, Targets, ast::not_<V>> {
+    template <class C>
+    CB_HD static word eval(const C& c) { return ~as_cond(ev<Dict, Targets, V>(c)); }
+};
+
+template <class Dict, class Targets, class L, class R>
+struct lower<Dict, Targets, ast::bit_and_<L, R>> {
+    template <class C>
+    CB_HD static auto eval(const C& c) {
+        auto a = ev<Dict, Targets, L>(c);
+        auto b = ev<Dict, Targets, R>(c);
+        if constexpr (std::is_same_v<decltype(a), word> && std::is_same_v<decltype(b), word>)
+            return word(a & b);
+        else
+            return band(as_planes(a), as_planes(b));
+    }
+};
+
+template <class Dict, class Targets, class L, class R>
+struct lower<Dict, Targets, ast::bit_or_<L, R>> {
+    template <class C>
+    CB_HD static auto eval(const C& c) {
+        auto a = ev<Dict, Targets, L>(c);
+        auto b = ev<Dict, Targets, R>(c);
+        if constexpr (std::is_same_v<decltype(a), word> && std::is_same_v<decltype(b), word>)
+            return word(a | b);
+        else
+            return bor(as_planes(a), as_planes(b));
+    }
+};
+
+template <class Dict, class Targets, class L, class R>
+struct lower<Dict, Targets, ast::plus<L, R>> {
+    template <class C>
+    CB_HD static auto eval(const C& c) {
+        return add(as_planes(ev<Dict, Targets, L>(c)), as_planes(ev<Dict, Targets, R>(c)));
+    }
+};
+
+template <class Dict, class Targets, class L, auto V>
+struct lower<Dict, Targets, ast::modulo<L, ast::constant<V>>> {
+    static_assert(V > 0 && (V & (V - 1)) == 0, "only modulo by a power of two is supported");
+    template <class C>
+    CB_HD static auto eval(const C& c) {
+        return resize<exact_log2(V)>(as_planes(ev<Dict, Targets, L>(c)));
+    }
+};
+
+#define CB_COMPARE(NODE, FN)                                                              \
+    template <class Dict, class Targets, class L, class R>                                \
+    struct lower<Dict, Targets, ast::NODE<L, R>> {                                        \
+        template <class C>                                                                \
+        CB_HD static word eval(const C& c) {                                              \
+            return FN(as_planes(ev<Dict, Targets, L>(c)), as_planes(ev<Dict, Targets, R>(c))); \
+        }                                                                                 \
+    };
+CB_COMPARE(equals, eq)
+CB_COMPARE(not_equals, ne)
+CB_COMPARE(greater_than, gt)
+CB_COMPARE(less_than, lt)
+#undef CB_COMPARE
+
+template <class Dict, class Targets, class V, int b>
+struct lower<Dict, Targets, ast::has_bit_set<V, b>> {
+    template <class C>
+    CB_HD static word eval(const C& c) {
+        auto v = as_planes(ev<Dict, Targets, V>(c));
+        static_assert(b >= 0 && b < decltype(v)::width, "has_bit_set bit beyond the value's width");
+        return v.p[b];
+    }
+};
+
+template <class Dict, class Targets, class Even, class Odd>
+struct lower<Dict, Targets, ast::alternate_algorithms<Even, Odd>> {
+    template <class RF, int TP>
+    CB_HD static auto eval(const ctx<RF, TP>& c) {
+        if constexpr (TP == 0)
+            return ev<Dict, Targets, Even>(c);
+        else
+            return ev<Dict, Targets, Odd>(c);
+    }
+};
+
+// Moore count of a fixed state: rows above and below contribute their 3-cell
+// sums, the own row its 2-cell sum; a 3-operand carry-save add gives 4 planes.
+template <class Dict, class Targets, auto V>
+struct lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>> {
+    static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
+    template <class C>
+    CB_HD static planes<4> eval(const C& c) {
+        const count_cache& a = c.up.cc[slot];
+        const count_cache& b = c.dn.cc[slot];
+        const count_cache& m = c.mid.cc[slot];
+        const word s0 = xor3(a.s3, b.s3, m.s2);
+        const word k1 = maj3(a.s3, b.s3, m.s2);
+        const word t1 = xor3(a.c3, b.c3, m.c2);
+        const word t2 = maj3(a.c3, b.c3, m.c2);
+        const word s1 = k1 ^ t1;
+        const word k2 = k1 & t1;
+        return planes<4>{{s0, s1, t2 ^ k2, t2 & k2}};
+    }
+};
+
+// von Neumann count of a fixed state: cells above and below plus the own row's
+// left+right sum; 3 planes.
+template <class Dict, class Targets, auto V>
+struct lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>> {
+    static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
+    template <class C>
+    CB_HD static planes<3> eval(const C& c) {
+        const word u = c.up.cc[slot].P[1], d = c.dn.cc[slot].P[1];
+        const count_cache& m = c.mid.cc[slot];
+        const word s0 = xor3(u, d, m.s2);
+        const word k1 = maj3(u, d, m.s2);
+        return planes<3>{{s0, m.c2 ^ k1, m.c2 & k1}};
+    }
+};
+
+// "any neighbour is S": a plain OR of the predicates (the count > 0 fast path
+// of include/evaluators/bit_planes.hpp:598-628, and its von Neumann analogue).
+template <class Dict, class Targets, auto V, auto Z>
+struct lower<Dict, Targets,
+             ast::greater_than<ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>, ast::constant<Z>>> {
+    static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
+    template <class C>
+    CB_HD static word eval(const C& c) {
+        if constexpr (Z == 0) {
+            const count_cache& a = c.up.cc[slot];
+            const count_cache& b = c.dn.cc[slot];
+            const count_cache& m = c.mid.cc[slot];
+            return a.P[0] | a.P[1] | a.P[2] | b.P[0] | b.P[1] | b.P[2] | m.P[0] | m.P[2];
+        } else {
+            return gt(lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>>::eval(c),
+                      from_constant<(long long)Z>());
+        }
+    }
+};
+
+template <class Dict, class Targets, auto V, auto Z>
+struct lower<Dict, Targets,
+             ast::greater_than<ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>,
+                               ast::constant<Z>>> {
+    static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
+    template <class C>
+    CB_HD static word eval(const C& c) {
+        if constexpr (Z == 0) {
+            return c.up.cc[slot].P[1] | c.dn.cc[slot].P[1] | c.mid.cc[slot].P[0] | c.mid.cc[slot].P[2];
+        } else {
+            return gt(lower<Dict, Targets,
+                            ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>>::eval(c),
+                      from_constant<(long long)Z>());
+        }
+    }
+};
+
+// Counts against a target that depends on the cell itself (e.g. cyclic's
+// (state + 1) mod 32): compare each neighbour's planes with the target.
+template <int NB, class T, class RF>
+CB_HD word neighbour_eq(const RF& row, int dxi, const T& target) {
+    planes<NB> n;
+#pragma unroll
+    for (int p = 0; p < NB; ++p) n.p[p] = row.sh[dxi][p];
+    return eq(n, target);
+}
+
+template <int N>
+CB_HD planes<4> popcount8(const word (&x)[N]) {
+    static_assert(N == 8);
+    // carry-save tree: 4 full adders + 3 half adders
+    const word a0 = xor3(x[0], x[1], x[2]), a1 = maj3(x[0], x[1], x[2]);
+    const word b0 = xor3(x[3], x[4], x[5]), b1 = maj3(x[3], x[4], x[5]);
+    const word c0 = xor3(x[6], x[7], a0), c1 = maj3(x[6], x[7], a0);
+    const word s0 = b0 ^ c0, d1 = b0 & c0;
+    const word e1 = xor3(a1, b1, c1), e2 = maj3(a1, b1, c1);
+    const word s1 = e1 ^ d1, f2 = e1 & d1;
+    return planes<4>{{s0, s1, e2 ^ f2, e2 & f2}};
+}
+
+template <class Dict, class Targets, class T>
+struct lower<Dict, Targets, ast::count_neighbors<T, ast::moore_8_neighbors>> {
+    static constexpr int NB = Dict::needed_bits;
+    template <class C>
+    CB_HD static planes<4> eval(const C& c) {
+        const auto t = as_planes(ev<Dict, Targets, T>(c));
+        const word x[8] = {neighbour_eq<NB>(c.up, 0, t),  neighbour_eq<NB>(c.up, 1, t),
+                           neighbour_eq<NB>(c.up, 2, t),  neighbour_eq<NB>(c.mid, 0, t),
+                           neighbour_eq<NB>(c.mid, 2, t), neighbour_eq<NB>(c.dn, 0, t),
+                           neighbour_eq<NB>(c.dn, 1, t),  neighbour_eq<NB>(c.dn, 2, t)};
+        return popcount8(x);
+    }
+};
+
+template <class Dict, class Targets, class T>
+struct lower<Dict, Targets, ast::count_neighbors<T, ast::von_neumann_4_neighbors>> {
+    static constexpr int NB = Dict::needed_bits;
+    template <class C>
+    CB_HD static planes<3> eval(const C& c) {
+        const auto t = as_planes(ev<Dict, Targets, T>(c));
+        const word u = neighbour_eq<NB>(c.up, 1, t), d = neighbour_eq<NB>(c.dn, 1, t);
+        const word l = neighbour_eq<NB>(c.mid, 0, t), r = neighbour_eq<NB>(c.mid, 2, t);
+        const word s0 = xor3(u, d, l), k1 = maj3(u, d, l);
+        const word s0b = s0 ^ r, k1b = s0 & r;
+        return planes<3>{{s0b, k1 ^ k1b, k1 & k1b}};
+    }
+};
+
+template <class Dict, class Targets, class T, auto Z>
+struct lower<Dict, Targets, ast::greater_than<ast::count_neighbors<T, ast::moore_8_neighbors>, ast::constant<Z>>> {
+    static constexpr int NB = Dict::needed_bits;
+    template <class C>
+    CB_HD static word eval(const C& c) {
+        if constexpr (Z == 0) {
+            const auto t = as_planes(ev<Dict, Targets, T>(c));
+            return neighbour_eq<NB>(c.up, 0, t) | neighbour_eq<NB>(c.up, 1, t) | neighbour_eq<NB>(c.up, 2, t) |
+                   neighbour_eq<NB>(c.mid, 0, t) | neighbour_eq<NB>(c.mid, 2, t) | neighbour_eq<NB>(c.dn, 0, t) |
+                   neighbour_eq<NB>(c.dn, 1, t) | neighbour_eq<NB>(c.dn, 2, t);
+        } else {
+            return gt(lower<Dict, Targets, ast::count_neighbors<T, ast::moore_8_neighbors>>::eval(c),
+                      from_constant<(long long)Z>());
+        }
+    }
+};
+
+// Margolus 2x2 block count of a fixed state (standard.hpp:175-205): the block
+// of a cell is itself, its horizontal partner, its vertical partner and the
+// diagonal one.  Per row, pair = P(x) + P(partner x); count = pair(own row) +
+// pair(partner row).
+template <class Dict, class Targets, auto V>
+struct lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::margolus_alternating_neighborhood>> {
+    static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
+    template <class RF, int TP>
+    CB_HD static planes<3> eval(const ctx<RF, TP>& c) {
+        constexpr word M = margolus_right_mask<TP>();
+        const count_cache& m = c.mid.cc[slot];
+        const count_cache& v = c.margolus_row().cc[slot];
+        const word hm = (m.P[2] & M) | (m.P[0] & ~M);
+        const word hv = (v.P[2] & M) | (v.P[0] & ~M);
+        const word a0 = m.P[1] ^ hm, a1 = m.P[1] & hm;
+        const word b0 = v.P[1] ^ hv, b1 = v.P[1] & hv;
+        const word k = a0 & b0;
+        return planes<3>{{a0 ^ b0, xor3(a1, b1, k), maj3(a1, b1, k)}};
+    }
+};
+
+// State of the diagonally opposite cell of the block (standard.hpp:207-241).
+template <class Dict, class Targets>
+struct lower<Dict, Targets, ast::margolus_180_neighbor> {
+    static constexpr int NB = Dict::needed_bits;
+    template <class RF, int TP>
+    CB_HD static planes<NB> eval(const ctx<RF, TP>& c) {
+        constexpr word M = margolus_right_mask<TP>();
+        const RF& v = c.margolus_row();
+        planes<NB> r;
+#pragma unroll
+        for (int p = 0; p < NB; ++p) r.p[p] = (v.sh[2][p] & M) | (v.sh[0][p] & ~M);
+        return r;
+    }
+};
+
+// ------------------------------------------------------------------ a rule
+// rule_net<Dict, Rule>: the lowered rule.  eval() returns the NB planes of
+// the next state of 32 cells; narrower results are zero-extended, wider ones
+// truncated to the stored planes (the extra planes of a valid state are zero).
+template <class Dict, class Rule>
+struct rule_net {
+    static constexpr int NB = Dict::needed_bits;
+    using targets = targets_of<Dict, Rule>;
+    using feat = row_feat<NB, targets>;
+
+    CB_HD static feat make_feat(const word* C, const word* L, const word* R) {
+        return make_row_feat<NB, targets>(C, L, R);
+    }
+
+    template <int TP>
+    CB_HD static void eval(const feat& up, const feat& mid, const feat& dn, int ypar, word* out) {
+        const ctx<feat, TP> c{up, mid, dn, ypar};
+        const auto r = as_planes(ev<Dict, targets, Rule>(c));
+        constexpr int B = decltype(r)::width;
+#pragma unroll
+        for (int p = 0; p < NB; ++p) out[p] = p < B ? r.p[p < B ? p : 0] : word(0);
+    }
+};
+
+}  // namespace cellato::b200
+
+#endif  // CELLATO_B200_LOWER_CUH

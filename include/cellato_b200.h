@@ -1,0 +1,144 @@
+/*
+ * cellato_b200.h -- C ABI of the B200 bit-plane hot path.
+ *
+ * The reference binds this path through C++ class templates (the grid,
+ * evaluator and traverser types picked by
+ * include/experiments/test_suites.hpp:115-225).  These entry points replace the
+ * device side of those templates behind plain pointers and sizes; the C++
+ * header shims in 2026-cellato-smpt-journal_b200/include/ (memory/,
+ * traversers/cuda/) call them so that the reference's callers compile
+ * unchanged.  Every function returns a cellato_status; none allocates unless
+ * its name says so, none frees caller memory, and all work is ordered on the
+ * given CUDA stream (0 = legacy default stream).
+ *
+ * Cells and layouts.  A grid of X x Y cells of an automaton with nb = needed
+ * bits is nb *planes*; plane i holds bit i of every cell's state-dictionary
+ * index.  Plane bytes are exactly the reference's:
+ *   CELLATO_LAYOUT_BIT_PLANES        include/memory/bit_planes_grid.hpp:234-270
+ *     words of W bits, word (x/W, y), bit x%W, least significant = leftmost;
+ *   CELLATO_LAYOUT_TILED_BIT_PLANES  include/memory/tiled_bit_planes_grid.hpp:243-288
+ *     words of 8 x (W/8) cells, bit (y%(W/8))*8 + x%8, tiles row-major.
+ * Each plane is X*Y/8 bytes, 16-byte aligned.  Accepted sizes: X a multiple of
+ * 32 (of 64 for W = 64 linear), Y >= 1 (a multiple of W/8 for tiled layouts).
+ * The reference's CUDA traversers accept a subset of these (they also need the
+ * word counts to divide the CUDA block and temporal tile,
+ * include/traversers/cuda/simple.hpp:45-49, temporal.hpp:60-86).
+ *
+ * Time.  Steps are numbered globally from t0; the parity of each step's number
+ * drives alternate_algorithms and the Margolus block phase exactly as the
+ * reference's time_step does (include/evaluators/standard.hpp:150-205).
+ */
+#ifndef CELLATO_B200_H
+#define CELLATO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* cellato_stream_t; /* == cudaStream_t */
+
+typedef enum {
+    CELLATO_OK = 0,
+    CELLATO_EINVAL = 1,        /* bad argument (null pointer, unknown id, ...) */
+    CELLATO_EINVAL_DIMS = 2,   /* grid sizes not accepted by the layout */
+    CELLATO_ESMEM = 3,         /* temporal tile does not fit in shared memory */
+    CELLATO_ECUDA = 4,         /* a CUDA runtime call failed; see cellato_last_error() */
+    CELLATO_ETIMEDOUT = 5,     /* a bounded device-side wait gave up */
+    CELLATO_ENOMEM = 6,        /* allocation failed */
+    CELLATO_EUNSUPPORTED = 7   /* combination not built */
+} cellato_status;
+
+typedef enum {
+    CELLATO_LAYOUT_BIT_PLANES = 0,
+    CELLATO_LAYOUT_TILED_BIT_PLANES = 1
+} cellato_layout;
+
+/* Rule ids: the ten automata of the reference (src/<automaton>/config.hpp). */
+typedef enum {
+    CELLATO_GAME_OF_LIFE = 0,
+    CELLATO_FOREST_FIRE = 1,
+    CELLATO_WIRE = 2,
+    CELLATO_EXCITABLE = 3,
+    CELLATO_BRIAN = 4,
+    CELLATO_MAZE = 5,
+    CELLATO_CYCLIC = 6,
+    CELLATO_FLUID = 7,
+    CELLATO_CRITTERS = 8,
+    CELLATO_TRAFFIC = 9,
+    CELLATO_RULE_COUNT = 10
+} cellato_rule;
+
+/* ---- identity ----------------------------------------------------------- */
+
+/* Library version string, e.g. "cellato-b200 1.0 sm_100a". */
+const char* cellato_version(void);
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* cellato_last_error(void);
+
+/* Rule id of a CLI automaton name ("game-of-life", "fire" or "forest-fire",
+ * ...; src/main.cpp:55-77), or -1. */
+int cellato_rule_from_name(const char* name);
+
+/* Name of a rule id (the config's `name`, e.g. "forest-fire"), or NULL. */
+const char* cellato_rule_name(int rule);
+
+/* needed_bits of the rule's state dictionary (state_dictionary.hpp:22), or -1. */
+int cellato_rule_planes(int rule);
+
+/* number_of_values of the rule's state dictionary, or -1. */
+int cellato_rule_states(int rule);
+
+/* Bytes of one plane of an X x Y grid (X*Y/8). */
+size_t cellato_plane_bytes(int x_cells, int y_cells);
+
+/* CELLATO_OK if (layout, word_bits, X, Y) is a grid shape this library runs. */
+int cellato_check_dims(int layout, int word_bits, int x_cells, int y_cells);
+
+/* ---- plane memory (replaces bit_planes_grid::to_cuda / to_cpu /
+ *      free_cuda_memory, bit_planes_grid.hpp:86-95, :132-168; same for the
+ *      tiled grid, tiled_bit_planes_grid.hpp:89-98, :141-177) ------------- */
+
+/* cudaMalloc nb planes of `bytes` each into planes_out[0..nb). */
+int cellato_planes_alloc(int nb, size_t bytes, void** planes_out);
+/* cudaFree nb planes (NULL entries are skipped) and clear the pointers. */
+int cellato_planes_free(int nb, void** planes);
+/* Stream-ordered copies of nb planes host -> device / device -> host. */
+int cellato_planes_upload(int nb, void* const* dev_planes, const void* const* host_planes, size_t bytes,
+                          cellato_stream_t stream);
+int cellato_planes_download(int nb, void* const* host_planes, const void* const* dev_planes, size_t bytes,
+                            cellato_stream_t stream);
+
+/* ---- traversers ----------------------------------------------------------- */
+
+/* Simple traverser (replaces include/traversers/cuda/simple.cu:43-87 with
+ * process_grid_kernel_simple :20-39): `steps` single-step launches, ping-pong
+ * between planes_a (input) and planes_b.  *result_in_b is set to 1 when the
+ * final state is in planes_b (odd number of launches), else 0.  Nothing is
+ * allocated; planes_a and planes_b must not overlap. */
+int cellato_run_simple(int rule, int layout, int word_bits, void* const* planes_a, void* const* planes_b,
+                       int x_cells, int y_cells, int t0, int steps, cellato_stream_t stream, int* result_in_b);
+
+/* Temporal traverser (replaces include/traversers/cuda/temporal.cu:137-272
+ * with process_grid_kernel_linear_temporal :35-135): launches of k fused steps
+ * each (the last launch takes the remainder), ping-pong as above.
+ * k in 1..32; tile_rows = rows of the shared-memory tile including the 2*k-row
+ * halo (0 = the library's choice for this rule/layout).  Returns CELLATO_ESMEM
+ * when the tile does not fit ("temporal tile is too large" in the reference,
+ * temporal.cu:214-216). */
+int cellato_run_temporal(int rule, int layout, int word_bits, void* const* planes_a, void* const* planes_b,
+                         int x_cells, int y_cells, int t0, int steps, int k, int tile_rows,
+                         cellato_stream_t stream, int* result_in_b);
+
+/* Largest tile_rows the temporal kernel accepts for (rule, layout, word_bits)
+ * on the current device, or a negative status. */
+int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CELLATO_B200_H */

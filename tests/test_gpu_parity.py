@@ -1,0 +1,104 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the golden
+fixtures (generated by the reference CPU standard path) and the oracle."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from cellato_b200 import inputs, lib
+
+from conftest import RULES
+
+pytestmark = pytest.mark.gpu
+
+# (layout, word_bits)
+LAYOUTS = [(0, 32), (0, 64), (1, 32), (1, 64)]
+
+
+def run_gpu(oracle, rule, layout, W, cells, steps, mode="simple", k=1, t0=0, tile_rows=0):
+    import torch
+    from cellato_b200.device import DevicePlanes
+    Y, X = cells.shape
+    nb = inputs.PLANES[rule]
+    a = DevicePlanes(nb, X, Y)
+    b = DevicePlanes(nb, X, Y)
+    a.upload(oracle.pack(layout, W, nb, cells))
+    if mode == "simple":
+        in_b = lib.run_simple(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps)
+    else:
+        in_b = lib.run_temporal(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps, k, tile_rows)
+    torch.cuda.synchronize()
+    res = (b if in_b else a).download()
+    return oracle.unpack(layout, W, nb, res, X, Y)
+
+
+@pytest.mark.parametrize("layout,W", LAYOUTS)
+def test_simple_small_golden(cuda, oracle, golden_small, layout, W):
+    for case, cin, cout in golden_small:
+        r = RULES.index(case["rule"])
+        out = run_gpu(oracle, r, layout, W, cin, case["steps"])
+        assert np.array_equal(out, cout), (case["key"], case["rule"], int((out != cout).sum()))
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 8, 16])
+@pytest.mark.parametrize("layout,W", LAYOUTS)
+def test_temporal_small_golden(cuda, oracle, golden_small, layout, W, k):
+    for case, cin, cout in golden_small:
+        r = RULES.index(case["rule"])
+        out = run_gpu(oracle, r, layout, W, cin, case["steps"], mode="temporal", k=k)
+        assert np.array_equal(out, cout), (case["key"], case["rule"], k, int((out != cout).sum()))
+
+
+@pytest.mark.parametrize("mode,k", [("simple", 1), ("temporal", 3), ("temporal", 8)])
+@pytest.mark.parametrize("t0", [1, 2, 7])
+def test_step_parity_offsets(cuda, oracle, mode, k, t0):
+    """alternate_algorithms and Margolus phase follow the global step number."""
+    rng = np.random.default_rng(t0)
+    for r in range(10):
+        cells = rng.integers(0, inputs.STATES[r], size=(40, 128), dtype=np.uint8)
+        want = oracle.run(r, cells, 11, t0=t0)
+        for layout, W in [(0, 32), (1, 64)]:
+            if layout == 1 and 40 % (W // 8):
+                continue
+            got = run_gpu(oracle, r, layout, W, cells, 11, mode=mode, k=k, t0=t0)
+            assert np.array_equal(got, want), (RULES[r], layout, W, t0)
+
+
+def test_odd_heights_and_narrow_rows(cuda, oracle):
+    """Ragged shapes: odd Y (linear), one-word rows, rows narrower than a warp."""
+    rng = np.random.default_rng(11)
+    for r in range(10):
+        for X, Y in [(32, 1), (32, 3), (64, 7), (96, 5), (160, 33), (4096, 9)]:
+            cells = rng.integers(0, inputs.STATES[r], size=(Y, X), dtype=np.uint8)
+            want = oracle.run(r, cells, 6)
+            assert np.array_equal(run_gpu(oracle, r, 0, 32, cells, 6), want), (RULES[r], X, Y)
+            assert np.array_equal(run_gpu(oracle, r, 0, 32, cells, 6, mode="temporal", k=4), want), (RULES[r], X, Y)
+
+
+def test_large_golden(cuda, oracle, golden_large):
+    """Workload-sized crops, full-grid SHA-256 against the reference's output."""
+    plans = {
+        "game-of-life": [(0, 64, "simple", 1), (0, 64, "temporal", 8), (1, 64, "temporal", 8)],
+        "wire": [(1, 64, "temporal", 8), (1, 64, "simple", 1), (1, 32, "temporal", 5)],
+        "excitable": [(1, 64, "temporal", 8), (1, 32, "simple", 1)],
+        "cyclic": [(0, 64, "simple", 1), (0, 32, "temporal", 4)],
+        "fluid": [(0, 64, "simple", 1), (0, 64, "temporal", 7), (1, 64, "temporal", 8)],
+    }
+    for case in golden_large:
+        rule = case["rule"]
+        r = RULES.index(rule)
+        if case["generator"] == "workload":
+            cells = inputs.workload_grid(rule, case["X"], case["Y"], case["seed"])
+        else:
+            cells = inputs.reference_density_grid(rule, case["X"], case["Y"], case["seed"])
+        for layout, W, mode, k in plans.get(rule, [(0, 64, "simple", 1), (1, 64, "temporal", 6)]):
+            out = run_gpu(oracle, r, layout, W, cells, case["steps"], mode=mode, k=k)
+            assert hashlib.sha256(out.tobytes()).hexdigest() == case["sha256_out"], (rule, layout, W, mode, k)
+
+
+def test_temporal_tile_too_large(cuda):
+    a = [0x1000]
+    b = [0x2000]
+    with pytest.raises(lib.CellatoError) as e:
+        lib.run_temporal("game-of-life", 0, 64, a, b, 64, 8, 0, 4, k=4, tile_rows=8 * 1000)
+    assert e.value.status == lib.ESMEM
