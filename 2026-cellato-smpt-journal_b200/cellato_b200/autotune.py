@@ -1,0 +1,114 @@
+"""Autotuner: picks the traverser configuration per automaton and grid size.
+
+The reference leaves (temporal_steps, temporal_tile_size_y, cuda_block_size_y)
+to the user and sweeps them with run_all.py (src/_scripts/cluster_run/
+run_all.py:9-24).  Here the choice is measured on the device: each candidate --
+the single-step kernel, or the temporal kernel with k fused steps -- runs a
+short burst on the caller's own device planes and the fastest per cell-step
+wins.  Results are cached per (rule, layout, word size, size class, device) in
+memory and in a JSON file, so a server or batch launcher pays the search once.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import threading
+
+from . import lib
+
+DEFAULT_CANDIDATES = (("simple", 1), ("temporal", 2), ("temporal", 4), ("temporal", 6), ("temporal", 8),
+                      ("temporal", 12), ("temporal", 16))
+
+_lock = threading.Lock()
+_memo: dict = {}
+
+
+def size_class(X: int, Y: int) -> int:
+    """log2 of the cell count, rounded: grids within a factor ~1.4 share a tuning."""
+    return int(round(math.log2(max(1, X * Y))))
+
+
+def cache_path() -> str:
+    return os.environ.get("CELLATO_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "cellato_b200_autotune.json"))
+
+
+def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
+    return f"{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+
+
+def _load_file() -> dict:
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store_file(key: str, value: dict) -> None:
+    try:
+        d = _load_file()
+        d[key] = value
+        os.makedirs(os.path.dirname(cache_path()), exist_ok=True)
+        tmp = cache_path() + f".{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
+            json.dump(d, f, indent=1)
+        os.replace(tmp, cache_path())
+    except OSError:
+        pass
+
+
+def run(choice: dict, rule: int, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int,
+        steps: int, stream: int = 0) -> int:
+    """Run `steps` steps with a tuned choice; returns 1 if the result is in planes_b."""
+    if choice["mode"] == "simple":
+        return lib.run_simple(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, stream)
+    return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
+                            choice.get("tile_rows", 0), stream)
+
+
+def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, candidates=DEFAULT_CANDIDATES,
+         burst_steps: int = 48, use_cache: bool = True) -> dict:
+    """Measure each candidate on (planes_a, planes_b) and return the fastest.
+
+    The planes are used as scratch: their content after tuning is some
+    evolution of the input.  Returns {"mode", "k", "tile_rows", "ns_per_cell_step"}.
+    """
+    import torch
+
+    rule = lib.rule_id(rule)
+    dev = torch.cuda.get_device_name(torch.cuda.current_device())
+    key = _key(rule, layout, word_bits, X, Y, dev)
+    if use_cache:
+        with _lock:
+            if key in _memo:
+                return _memo[key]
+            disk = _load_file().get(key)
+            if disk:
+                _memo[key] = disk
+                return disk
+    best = None
+    stream = torch.cuda.current_stream().cuda_stream
+    for mode, k in candidates:
+        choice = {"mode": mode, "k": k, "tile_rows": 0}
+        steps = max(burst_steps, 2 * k) // k * k
+        try:
+            run(choice, rule, layout, word_bits, planes_a, planes_b, X, Y, 0, k, stream)  # warm-up
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run(choice, rule, layout, word_bits, planes_a, planes_b, X, Y, 0, steps, stream)
+            e1.record()
+            e1.synchronize()
+        except lib.CellatoError:
+            continue
+        ns = e0.elapsed_time(e1) * 1e6 / (X * Y * steps)
+        if best is None or ns < best["ns_per_cell_step"]:
+            best = dict(choice, ns_per_cell_step=ns)
+    if best is None:
+        raise RuntimeError("no autotune candidate ran")
+    if use_cache:
+        with _lock:
+            _memo[key] = best
+        _store_file(key, best)
+    return best

@@ -44,3 +44,15 @@ class DevicePlanes:
         for p in range(self.nb):
             out[p] = self.view(p).cpu().numpy()
         return out
+
+    # ---- device packing (C ABI cellato_pack_cells / cellato_unpack_cells)
+    def pack_from(self, cells: torch.Tensor, layout: int, word_bits: int, stream: int = 0) -> None:
+        """cells: (Y, X) uint8 CUDA tensor of state indices."""
+        assert cells.dtype == torch.uint8 and cells.is_cuda and cells.is_contiguous()
+        assert tuple(cells.shape) == (self.Y, self.X)
+        lib.pack_cells(layout, word_bits, self.nb, cells.data_ptr(), self.X, self.Y, self.ptrs, stream)
+
+    def unpack(self, layout: int, word_bits: int, stream: int = 0) -> torch.Tensor:
+        cells = torch.empty((self.Y, self.X), dtype=torch.uint8, device=self.buf.device)
+        lib.unpack_cells(layout, word_bits, self.nb, self.ptrs, self.X, self.Y, cells.data_ptr(), stream)
+        return cells

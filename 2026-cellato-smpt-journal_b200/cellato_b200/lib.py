@@ -25,6 +25,7 @@ EXPORTED = [
     "cellato_version", "cellato_last_error", "cellato_rule_from_name", "cellato_rule_name",
     "cellato_rule_planes", "cellato_rule_states", "cellato_plane_bytes", "cellato_check_dims",
     "cellato_planes_alloc", "cellato_planes_free", "cellato_planes_upload", "cellato_planes_download",
+    "cellato_pack_cells", "cellato_unpack_cells",
     "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
 ]
 
@@ -60,6 +61,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     i = ctypes.c_int
     lib.cellato_run_simple.argtypes = [i, i, i, _PP, _PP, i, i, i, i, _vp, ctypes.POINTER(i)]
     lib.cellato_run_temporal.argtypes = [i, i, i, _PP, _PP, i, i, i, i, i, i, _vp, ctypes.POINTER(i)]
+    lib.cellato_pack_cells.argtypes = [i, i, i, _vp, i, i, _PP, _vp]
+    lib.cellato_unpack_cells.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
     _lib = lib
     return lib
 
@@ -104,6 +107,16 @@ def run_simple(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y:
     check(load().cellato_run_simple(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),
                                     X, Y, t0, steps, stream, ctypes.byref(out)))
     return out.value
+
+
+def pack_cells(layout: int, word_bits: int, nb: int, cells_ptr: int, X: int, Y: int, planes, stream: int = 0) -> None:
+    """Device uint8 cells (row-major) -> nb device planes."""
+    check(load().cellato_pack_cells(layout, word_bits, nb, cells_ptr, X, Y, ptr_array(planes), stream))
+
+
+def unpack_cells(layout: int, word_bits: int, nb: int, planes, X: int, Y: int, cells_ptr: int, stream: int = 0) -> None:
+    """nb device planes -> device uint8 cells (row-major)."""
+    check(load().cellato_unpack_cells(layout, word_bits, nb, ptr_array(planes), X, Y, cells_ptr, stream))
 
 
 def run_temporal(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,

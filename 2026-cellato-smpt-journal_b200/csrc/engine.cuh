@@ -177,13 +177,26 @@ __device__ __forceinline__ void build_feat(const word (&C)[NB][V], const word (&
 // ======================================================= single-step kernel
 // One launch = one time step.  Each warp owns a horizontal segment of 32*V
 // words (lane l: words seg*32V + l*V .. +V-1) and walks down the CTA's rows in
-// bands of R rows with a rolling window of three rows' features; every input
+// bands of BR rows with a rolling window of three rows' features.  The next
+// band's loads are issued before the current band is computed, so a warp keeps
+// BR rows x NB planes x 32V words in flight (the single-step kernel streams:
+// HBM latency x bandwidth must be covered by bytes in flight).  Every input
 // word is loaded once per CTA row range (+2 halo rows), every output word
 // stored once.
+//   linear : BR = SIMPLE_LINEAR_BAND independent rows per band
+//   tiled  : BR = rows of one tile word (4 or 8)
+constexpr int SIMPLE_LINEAR_BAND = 8;
+
+template <int LAYOUT>
+constexpr int simple_band_rows() {
+    return LAYOUT == LAYOUT_LINEAR ? SIMPLE_LINEAR_BAND : band_rows<LAYOUT>();
+}
+
 template <class Net, int NB, int LAYOUT, int V, int TP, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, plane_set out, int Xw, int Yb,
-                                                                 int Y, int bands_per_cta) {
+__global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, plane_set out, int Xw, int Y,
+                                                                 int nbands, int bands_per_cta) {
     constexpr int R = band_rows<LAYOUT>();
+    constexpr int BR = simple_band_rows<LAYOUT>();
     using feat = typename Net::feat;
     const int lane = threadIdx.x & 31;
     const int seg = blockIdx.x * WARPS + (threadIdx.x >> 5);
@@ -192,99 +205,160 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
     const int gx = gx_raw % Xw;
     const int gx_left = (seg * 32 * V + Xw - 1) % Xw;     // word left of the segment
     const int gx_right = (seg * 32 * V + 32 * V) % Xw;    // word right of the segment
-    const bool seg_spans_row = (32 * V == Xw);  // lane 0 / 31 neighbours are lanes 31 / 0
+    const bool seg_spans_row = (32 * V == Xw);            // lane 0 / 31 neighbours are lanes 31 / 0
 
     const int b0 = blockIdx.y * bands_per_cta;
-    const int b1 = min(Yb, b0 + bands_per_cta);
+    const int b1 = min(nbands, b0 + bands_per_cta);
     if (b0 >= b1) return;
 
-    auto load_band = [&](int b, word (&raw)[R][NB][V], word (&L)[R][NB], word (&Rr)[R][NB]) {
-        const int bw = (b % Yb + Yb) % Yb;
+    // Load one band: linear -> rows b*BR .. b*BR+BR-1 (wrapped), tiled -> tile row b.
+    auto load_band = [&](int b, word (&raw)[BR][NB][V], word (&L)[BR][NB], word (&Rr)[BR][NB]) {
+        if constexpr (LAYOUT == LAYOUT_LINEAR) {
+            int y = (b * BR) % Y;
+            if (y < 0) y += Y;
 #pragma unroll
-        for (int p = 0; p < NB; ++p) {
-            word rows[R][V];
-            load_lane<LAYOUT, V>(in.p[p], Xw, bw, gx, rows);
+            for (int r = 0; r < BR; ++r) {
 #pragma unroll
-            for (int r = 0; r < R; ++r)
+                for (int p = 0; p < NB; ++p) {
+                    word rows[1][V];
+                    load_lane<LAYOUT, V>(in.p[p], Xw, y, gx, rows);
 #pragma unroll
-                for (int v = 0; v < V; ++v) raw[r][p][v] = rows[r][v];
-        }
+                    for (int v = 0; v < V; ++v) raw[r][p][v] = rows[0][v];
+                }
+                if (!seg_spans_row && (lane == 0 || lane == 31)) {
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int p = 0; p < NB; ++p) {
-                L[r][p] = from_left_lane(raw[r][p][V - 1]);
-                Rr[r][p] = from_right_lane(raw[r][p][0]);
+                    for (int p = 0; p < NB; ++p) {
+                        const word e = __ldg(in.p[p] + (size_t)y * Xw + (lane == 0 ? gx_left : gx_right));
+                        if (lane == 0) L[r][p] = e; else Rr[r][p] = e;
+                    }
+                }
+                if (++y == Y) y = 0;
             }
-        if (!seg_spans_row && (lane == 0 || lane == 31)) {
-            const int gxe = lane == 0 ? gx_left : gx_right;
+        } else {
+            int bw = b % nbands;
+            if (bw < 0) bw += nbands;
 #pragma unroll
             for (int p = 0; p < NB; ++p) {
-                word rows[R];
-                load_word_rows<LAYOUT>(in.p[p], Xw, bw, gxe, rows);
+                word rows[R][V];
+                load_lane<LAYOUT, V>(in.p[p], Xw, bw, gx, rows);
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    if (lane == 0)
-                        L[r][p] = rows[r];
-                    else
-                        Rr[r][p] = rows[r];
+                for (int r = 0; r < R; ++r)
+#pragma unroll
+                    for (int v = 0; v < V; ++v) raw[r][p][v] = rows[r][v];
+            }
+            if (!seg_spans_row && (lane == 0 || lane == 31)) {
+                const int gxe = lane == 0 ? gx_left : gx_right;
+#pragma unroll
+                for (int p = 0; p < NB; ++p) {
+                    word rows[R];
+                    load_word_rows<LAYOUT>(in.p[p], Xw, bw, gxe, rows);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        if (lane == 0) L[r][p] = rows[r]; else Rr[r][p] = rows[r];
+                    }
                 }
             }
         }
     };
-
-    word cur[R][NB][V], curL[R][NB], curR[R][NB];
-    word nxt[R][NB][V], nxtL[R][NB], nxtR[R][NB];
-    feat up[V], mid[V], dn[V];
-
-    // row above the first band: last row of the previous band
-    load_band(b0 - 1, nxt, nxtL, nxtR);
-    {
-        word C[NB][V], Lw[NB], Rw[NB];
+    // neighbour words from the adjacent lanes (edge lanes keep their loads)
+    auto link_lanes = [&](const word (&raw)[BR][NB][V], word (&L)[BR][NB], word (&Rr)[BR][NB]) {
 #pragma unroll
-        for (int p = 0; p < NB; ++p) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) C[p][v] = nxt[R - 1][p][v];
-            Lw[p] = nxtL[R - 1][p];
-            Rw[p] = nxtR[R - 1][p];
-        }
-        build_feat<Net, NB, V>(C, Lw, Rw, up);
-    }
-    load_band(b0, cur, curL, curR);
-    {
-        word C[NB][V], Lw[NB], Rw[NB];
-#pragma unroll
-        for (int p = 0; p < NB; ++p) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) C[p][v] = cur[0][p][v];
-            Lw[p] = curL[0][p];
-            Rw[p] = curR[0][p];
-        }
-        build_feat<Net, NB, V>(C, Lw, Rw, mid);
-    }
-
-    for (int b = b0; b < b1; ++b) {
-        load_band(b + 1, nxt, nxtL, nxtR);
-        word res[R][NB][V];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            word C[NB][V], Lw[NB], Rw[NB];
+        for (int r = 0; r < BR; ++r)
 #pragma unroll
             for (int p = 0; p < NB; ++p) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) C[p][v] = r + 1 < R ? cur[r + 1 < R ? r + 1 : 0][p][v] : nxt[0][p][v];
-                Lw[p] = r + 1 < R ? curL[r + 1 < R ? r + 1 : 0][p] : nxtL[0][p];
-                Rw[p] = r + 1 < R ? curR[r + 1 < R ? r + 1 : 0][p] : nxtR[0][p];
+                const word l = from_left_lane(raw[r][p][V - 1]);
+                const word rr = from_right_lane(raw[r][p][0]);
+                if (seg_spans_row || lane != 0) L[r][p] = l;
+                if (seg_spans_row || lane != 31) Rr[r][p] = rr;
             }
-            build_feat<Net, NB, V>(C, Lw, Rw, dn);
-            const int y = b * R + r;
-            const int ypar = (y < Y ? y : y - Y) & 1;
+    };
+    auto feat_of = [&](const word (&raw)[BR][NB][V], const word (&L)[BR][NB], const word (&Rr)[BR][NB], int r,
+                       feat (&f)[V]) {
+        word C[NB][V], Lw[NB], Rw[NB];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) C[p][v] = raw[r][p][v];
+            Lw[p] = L[r][p];
+            Rw[p] = Rr[r][p];
+        }
+        build_feat<Net, NB, V>(C, Lw, Rw, f);
+    };
+
+    word cur[BR][NB][V], curL[BR][NB], curR[BR][NB];
+    word nxt[BR][NB][V], nxtL[BR][NB], nxtR[BR][NB];
+    feat up[V], mid[V], dn[V];
+
+    // the row above the first band
+    if constexpr (LAYOUT == LAYOUT_LINEAR) {
+        int y = (b0 * BR - 1) % Y;
+        if (y < 0) y += Y;
+        word C[NB][V], Lw[NB], Rw[NB];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            word rows[1][V];
+            load_lane<LAYOUT, V>(in.p[p], Xw, y, gx, rows);
+#pragma unroll
+            for (int v = 0; v < V; ++v) C[p][v] = rows[0][v];
+            Lw[p] = 0;
+            Rw[p] = 0;
+            if (!seg_spans_row && (lane == 0 || lane == 31)) {
+                const word e = __ldg(in.p[p] + (size_t)y * Xw + (lane == 0 ? gx_left : gx_right));
+                if (lane == 0) Lw[p] = e; else Rw[p] = e;
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            const word l = from_left_lane(C[p][V - 1]);
+            const word r = from_right_lane(C[p][0]);
+            if (seg_spans_row || lane != 0) Lw[p] = l;
+            if (seg_spans_row || lane != 31) Rw[p] = r;
+        }
+        build_feat<Net, NB, V>(C, Lw, Rw, up);
+    } else {
+        load_band(b0 - 1, nxt, nxtL, nxtR);
+        link_lanes(nxt, nxtL, nxtR);
+        feat_of(nxt, nxtL, nxtR, BR - 1, up);
+    }
+    load_band(b0, cur, curL, curR);
+    link_lanes(cur, curL, curR);
+    feat_of(cur, curL, curR, 0, mid);
+
+    for (int b = b0; b < b1; ++b) {
+        load_band(b + 1, nxt, nxtL, nxtR);  // in flight while this band computes
+        word res[LAYOUT == LAYOUT_LINEAR ? 1 : BR][NB][V];
+#pragma unroll
+        for (int r = 0; r < BR; ++r) {
+            if (r + 1 < BR) {
+                feat_of(cur, curL, curR, r + 1 < BR ? r + 1 : 0, dn);
+            } else {
+                link_lanes(nxt, nxtL, nxtR);
+                feat_of(nxt, nxtL, nxtR, 0, dn);
+            }
+            const int y = b * BR + r;
+            word o[NB][V];
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                word o[NB];
-                Net::template eval<TP>(up[v], mid[v], dn[v], ypar, o);
+                word ov[NB];
+                Net::template eval<TP>(up[v], mid[v], dn[v], y & 1, ov);
 #pragma unroll
-                for (int p = 0; p < NB; ++p) res[r][p][v] = o[p];
+                for (int p = 0; p < NB; ++p) o[p][v] = ov[p];
+            }
+            if constexpr (LAYOUT == LAYOUT_LINEAR) {
+                if (owns && y < Y) {
+#pragma unroll
+                    for (int p = 0; p < NB; ++p) {
+                        word rows[1][V];
+#pragma unroll
+                        for (int v = 0; v < V; ++v) rows[0][v] = o[p][v];
+                        store_lane<LAYOUT, V>(out.p[p], Xw, y, gx, rows);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int p = 0; p < NB; ++p)
+#pragma unroll
+                    for (int v = 0; v < V; ++v) res[r < BR ? r : 0][p][v] = o[p][v];
             }
 #pragma unroll
             for (int v = 0; v < V; ++v) {
@@ -292,19 +366,21 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
                 mid[v] = dn[v];
             }
         }
-        if (owns) {
+        if constexpr (LAYOUT != LAYOUT_LINEAR) {
+            if (owns) {
 #pragma unroll
-            for (int p = 0; p < NB; ++p) {
-                word rows[R][V];
+                for (int p = 0; p < NB; ++p) {
+                    word rows[R][V];
 #pragma unroll
-                for (int r = 0; r < R; ++r)
+                    for (int r = 0; r < R; ++r)
 #pragma unroll
-                    for (int v = 0; v < V; ++v) rows[r][v] = res[r][p][v];
-                store_lane<LAYOUT, V>(out.p[p], Xw, b, gx, rows);
+                        for (int v = 0; v < V; ++v) rows[r][v] = res[r][p][v];
+                    store_lane<LAYOUT, V>(out.p[p], Xw, b, gx, rows);
+                }
             }
         }
 #pragma unroll
-        for (int r = 0; r < R; ++r)
+        for (int r = 0; r < BR; ++r)
 #pragma unroll
             for (int p = 0; p < NB; ++p) {
 #pragma unroll
@@ -416,8 +492,30 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
         }
     };
 
-    auto step = [&](int t, auto tp_tag) {
+    // One output row r: dn features from row r+1 (or the saved bottom row),
+    // evaluation, in-place write.  fu/fm/fd rotate roles between calls.
+    auto row_body = [&](int r, int hi, int gy, const feat (&fu)[V], const feat (&fm)[V], feat (&fd)[V],
+                        const word (&botC)[NB][V], const word (&botL)[NB], const word (&botR)[NB], auto tp_tag) {
         constexpr int TP = decltype(tp_tag)::value;
+        if (r + 1 < hi) {
+            word C[NB][V], L[NB], Rr[NB];
+            read_row(r + 1, C, L, Rr);
+            build_feat<Net, NB, V>(C, L, Rr, fd);
+        } else {
+            build_feat<Net, NB, V>(botC, botL, botR, fd);
+        }
+        word o[NB][V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            word ov[NB];
+            Net::template eval<TP>(fu[v], fm[v], fd[v], gy & 1, ov);
+#pragma unroll
+            for (int p = 0; p < NB; ++p) o[p][v] = ov[p];
+        }
+        write_row(r, o);
+    };
+
+    auto step = [&](int t, auto tp_tag) {
         const int lo = max(rw0, t);
         const int hi = min(rw1, TH - t);
         word topC[NB][V], topL[NB], topR[NB], botC[NB][V], botL[NB], botR[NB];
@@ -427,36 +525,31 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
         }
         __syncthreads();
         if (lo < hi) {
-            feat up[V], mid[V], dn[V];
-            build_feat<Net, NB, V>(topC, topL, topR, up);
+            feat fa[V], fb[V], fc[V];
+            build_feat<Net, NB, V>(topC, topL, topR, fa);
             {
                 word C[NB][V], L[NB], Rr[NB];
                 read_row(lo, C, L, Rr);
-                build_feat<Net, NB, V>(C, L, Rr, mid);
+                build_feat<Net, NB, V>(C, L, Rr, fb);
             }
-            for (int r = lo; r < hi; ++r) {
-                if (r + 1 < hi) {
-                    word C[NB][V], L[NB], Rr[NB];
-                    read_row(r + 1, C, L, Rr);
-                    build_feat<Net, NB, V>(C, L, Rr, dn);
-                } else {
-                    build_feat<Net, NB, V>(botC, botL, botR, dn);
-                }
-                const int gy = ((y0 - HY + r) % Y + Y) % Y;
-                word o[NB][V];
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    word ov[NB];
-                    Net::template eval<TP>(up[v], mid[v], dn[v], gy & 1, ov);
-#pragma unroll
-                    for (int p = 0; p < NB; ++p) o[p][v] = ov[p];
-                }
-                write_row(r, o);
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    up[v] = mid[v];
-                    mid[v] = dn[v];
-                }
+            // global row of tile row lo, advanced incrementally (no division per row)
+            int gy = (y0 - HY + lo) % Y;
+            if (gy < 0) gy += Y;
+            auto next_gy = [&](int g) { return g + 1 == Y ? 0 : g + 1; };
+            int r = lo;
+            // three rows per trip: the feature buffers rotate by name, not by copy
+            for (; r + 3 <= hi; r += 3) {
+                row_body(r, hi, gy, fa, fb, fc, botC, botL, botR, tp_tag);
+                gy = next_gy(gy);
+                row_body(r + 1, hi, gy, fb, fc, fa, botC, botL, botR, tp_tag);
+                gy = next_gy(gy);
+                row_body(r + 2, hi, gy, fc, fa, fb, botC, botL, botR, tp_tag);
+                gy = next_gy(gy);
+            }
+            if (r < hi) {
+                row_body(r, hi, gy, fa, fb, fc, botC, botL, botR, tp_tag);
+                gy = next_gy(gy);
+                if (r + 1 < hi) row_body(r + 1, hi, gy, fb, fc, fa, botC, botL, botR, tp_tag);
             }
         }
         __syncthreads();

@@ -32,11 +32,12 @@ struct rule_ops {
 // Words per lane of the single-step kernel: as wide as registers allow.  A row
 // of features costs about 3 words per plane plus 5 per count target per lane
 // word, and three rows plus three bands of raw words are live.
-template <class Net, int NB, int R>
+template <class Net, int NB, int LAYOUT>
 constexpr int simple_words_per_lane() {
+    constexpr int BR = simple_band_rows<LAYOUT>();
     constexpr int feat_words = 3 * NB + 5 * Net::targets::size;
-    constexpr int per_v = 3 * feat_words + 3 * R * NB;
-    return per_v * 4 <= 128 ? 4 : (per_v * 2 <= 128 ? 2 : 1);
+    constexpr int per_v = 3 * feat_words + 2 * BR * NB + (LAYOUT == LAYOUT_LINEAR ? 0 : BR * NB);
+    return per_v * 4 <= 160 ? 4 : (per_v * 2 <= 160 ? 2 : 1);
 }
 
 template <class A>
@@ -51,27 +52,26 @@ struct rule_kernels {
 
     template <int LAYOUT, int V>
     static cudaError_t simple_v(const plane_set& in, const plane_set& out, int Xw, int Y, int t, cudaStream_t s) {
-        constexpr int R = band_rows<LAYOUT>();
-        const int Yb = Y / R;
+        constexpr int BR = simple_band_rows<LAYOUT>();
+        const int nbands = (Y + BR - 1) / BR;
         const int segments = (Xw + 32 * V - 1) / (32 * V);
         const int cta_x = (segments + SIMPLE_WARPS - 1) / SIMPLE_WARPS;
         // enough warps to cover 148 SMs x 32 resident warps, at most 64 rows per CTA
-        long long want = 148LL * 32;
-        int bands = (int)std::max(1LL, std::min<long long>(64 / R, (long long)segments * Yb / want));
-        bands = std::max(1, bands);
-        const int cta_y = (Yb + bands - 1) / bands;
+        const long long want = 148LL * 32;
+        const int bands = (int)std::max(1LL, std::min<long long>(std::max(1, 64 / BR), (long long)segments * nbands / want));
+        const int cta_y = (nbands + bands - 1) / bands;
         const dim3 grid(cta_x, cta_y), block(SIMPLE_WARPS * 32);
         if (t & 1)
-            simple_step_kernel<net, NB, LAYOUT, V, 1, SIMPLE_WARPS><<<grid, block, 0, s>>>(in, out, Xw, Yb, Y, bands);
+            simple_step_kernel<net, NB, LAYOUT, V, 1, SIMPLE_WARPS><<<grid, block, 0, s>>>(in, out, Xw, Y, nbands, bands);
         else
-            simple_step_kernel<net, NB, LAYOUT, V, 0, SIMPLE_WARPS><<<grid, block, 0, s>>>(in, out, Xw, Yb, Y, bands);
+            simple_step_kernel<net, NB, LAYOUT, V, 0, SIMPLE_WARPS><<<grid, block, 0, s>>>(in, out, Xw, Y, nbands, bands);
         return cudaGetLastError();
     }
 
     template <int LAYOUT>
     static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t,
                                      cudaStream_t s) {
-        constexpr int VMAX = simple_words_per_lane<net, NB, band_rows<LAYOUT>()>();
+        constexpr int VMAX = simple_words_per_lane<net, NB, LAYOUT>();
         if constexpr (VMAX >= 4)
             if (Xw % 4 == 0) return simple_v<LAYOUT, 4>(in, out, Xw, Y, t, s);
         if constexpr (VMAX >= 2)

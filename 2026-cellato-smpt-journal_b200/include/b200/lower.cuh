@@ -394,9 +394,11 @@ struct ctx {
         else
             return mid;
     }
-    // Row holding the vertical Margolus partner: y+1 when (y + t) is even,
-    // y-1 otherwise (include/evaluators/standard.hpp:183-197).
-    CB_HD const RF& margolus_row() const { return ((ypar ^ TP) == 0) ? dn : up; }
+    // The vertical Margolus partner of the output row is y+1 when (y + t) is
+    // even and y-1 otherwise (include/evaluators/standard.hpp:183-197).  The
+    // choice is made per word value (a select), never by picking a struct.
+    CB_HD bool margolus_down() const { return ((ypar ^ TP) == 0); }
+    CB_HD word pick(word down_value, word up_value) const { return margolus_down() ? down_value : up_value; }
 };
 
 // Bits whose horizontal Margolus partner is x+1: even x on even steps, odd x
@@ -717,11 +719,13 @@ struct lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::ma
     CB_HD static planes<3> eval(const ctx<RF, TP>& c) {
         constexpr word M = margolus_right_mask<TP>();
         const count_cache& m = c.mid.cc[slot];
-        const count_cache& v = c.margolus_row().cc[slot];
+        const count_cache& u = c.up.cc[slot];
+        const count_cache& d = c.dn.cc[slot];
+        const word v0 = c.pick(d.P[0], u.P[0]), v1 = c.pick(d.P[1], u.P[1]), v2 = c.pick(d.P[2], u.P[2]);
         const word hm = (m.P[2] & M) | (m.P[0] & ~M);
-        const word hv = (v.P[2] & M) | (v.P[0] & ~M);
+        const word hv = (v2 & M) | (v0 & ~M);
         const word a0 = m.P[1] ^ hm, a1 = m.P[1] & hm;
-        const word b0 = v.P[1] ^ hv, b1 = v.P[1] & hv;
+        const word b0 = v1 ^ hv, b1 = v1 & hv;
         const word k = a0 & b0;
         return planes<3>{{a0 ^ b0, xor3(a1, b1, k), maj3(a1, b1, k)}};
     }
@@ -734,10 +738,13 @@ struct lower<Dict, Targets, ast::margolus_180_neighbor> {
     template <class RF, int TP>
     CB_HD static planes<NB> eval(const ctx<RF, TP>& c) {
         constexpr word M = margolus_right_mask<TP>();
-        const RF& v = c.margolus_row();
         planes<NB> r;
 #pragma unroll
-        for (int p = 0; p < NB; ++p) r.p[p] = (v.sh[2][p] & M) | (v.sh[0][p] & ~M);
+        for (int p = 0; p < NB; ++p) {
+            const word right = c.pick(c.dn.sh[2][p], c.up.sh[2][p]);
+            const word left = c.pick(c.dn.sh[0][p], c.up.sh[0][p]);
+            r.p[p] = (right & M) | (left & ~M);
+        }
         return r;
     }
 };

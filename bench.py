@@ -1,0 +1,414 @@
+"""Benchmark of the B200 bit-plane hot path.
+
+Workload (one bench step): WireWorld and Greenberg-Hastings (the `excitable`
+automaton), each on one 16384 x 16384 torus in the tiled_bit_planes layout
+with 64-bit words, advanced 1000 steps each; the traverser (single-step or
+temporal with k fused steps) is chosen per automaton by the autotuner.
+Inputs are seeded synthetic grids: WireWorld i.i.d. empty/conductor/head/tail
+= .50/.40/.05/.05, Greenberg-Hastings uniform over its 8 states.
+
+Metric: GCUPS = cell updates / s / 1e9, summed over both automata and all
+ranks.  `value` times the work with the planes resident in HBM; `e2e` times the
+same work through the C ABI with host buffers: every step uploads both grids'
+input planes from pinned host memory, runs, and downloads the result planes.
+
+The ping-pong plane buffers (WireWorld 128 MiB, Greenberg-Hastings 192 MiB)
+exceed the 126 MB L2, so no L2 flush is inserted between steps.
+
+Usage:
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 run under torch.distributed.run: every rank runs the same workload on
+its own GPU (replicas: the path has no exchange step) and rank 0 reports the
+sum of cell updates over the maximum per-rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "2026-cellato-smpt-journal_b200")
+sys.path.insert(0, PKG)
+
+AUTOMATA = ("wire", "excitable")
+SIZE = 16384
+CA_STEPS = 1000
+LAYOUT = 1        # tiled_bit_planes
+WORD_BITS = 64
+SEED = 42
+CPU_SAMPLE_SIZE = 2048
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--ca-steps", type=int, default=CA_STEPS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.samples = []
+        if self.proc is None:
+            return False
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+        return False
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return None
+
+        sm = [num(s[1]) for s in self.samples if num(s[1]) is not None]
+        mx = [num(s[2]) for s in self.samples if num(s[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        sm_sorted = sorted(sm)
+        load = [v for v in sm_sorted if v >= 0.5 * max(sm_sorted)] if sm_sorted else []
+        med = load[len(load) // 2] if load else None
+        return {"sm_mhz": med, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples),
+                "power_w_max": max((num(s[3]) or 0.0) for s in self.samples)}
+
+
+# --------------------------------------------------------- reference arm
+def load_reference_cpu():
+    """The reference's own CPU path (oracle/_ref) when it was built from the
+    reference tree, else the oracle's C restatement of it."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle, RefOracle
+    try:
+        ref = RefOracle()
+        return "reference", (lambda r, c, s, th: ref.run_standard(r, c, s, threads=th))
+    except FileNotFoundError:
+        o = Oracle()
+        return "port", (lambda r, c, s, th: o.run(r, c, s, threads=th))
+
+
+def cpu_sample(run, threads: int, target_s: float):
+    """Time the CPU standard path on CPU_SAMPLE_SIZE^2 crops of both automata,
+    sized to about target_s seconds.  Returns (GCUPS, description)."""
+    from cellato_b200 import inputs
+    n = CPU_SAMPLE_SIZE
+    grids = {a: inputs.workload_grid(a, n, n, SEED) for a in AUTOMATA}
+    t = time.perf_counter()
+    for a in AUTOMATA:
+        run(inputs.RULE_ID[a], grids[a], 4, threads)
+    probe = time.perf_counter() - t
+    steps = max(4, int(4 * target_s / max(probe, 1e-3)))
+    t = time.perf_counter()
+    for a in AUTOMATA:
+        run(inputs.RULE_ID[a], grids[a], steps, threads)
+    dt = time.perf_counter() - t
+    cells = len(AUTOMATA) * n * n * steps
+    return cells / dt / 1e9, f"{'+'.join(AUTOMATA)} {n}x{n} crops, {steps} steps each, {dt:.1f} s"
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return
+    kind, run = load_reference_cpu()
+    threads = host_threads()
+    from cellato_b200 import inputs
+    n = CPU_SAMPLE_SIZE
+    grids = {a: inputs.workload_grid(a, n, n, SEED) for a in AUTOMATA}
+    # size one step to ~4 s of work so the whole run stays within a few minutes
+    t = time.perf_counter()
+    for a in AUTOMATA:
+        run(inputs.RULE_ID[a], grids[a], 2, threads)
+    per_ca_step = (time.perf_counter() - t) / 2
+    ca_steps = max(2, int(4.0 / max(per_ca_step, 1e-4)))
+    for _ in range(args.warmup):
+        for a in AUTOMATA:
+            run(inputs.RULE_ID[a], grids[a], max(1, ca_steps // 8), threads)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        for a in AUTOMATA:
+            run(inputs.RULE_ID[a], grids[a], ca_steps, threads)
+    dt = time.perf_counter() - t
+    cells = args.steps * len(AUTOMATA) * n * n * ca_steps
+    value = cells / dt / 1e9
+    sample = f"each step: {'+'.join(AUTOMATA)} {n}x{n} crops x {ca_steps} steps, CPU standard evaluator"
+    line = {
+        "impl": "reference", "metric": "GCUPS", "value": round(value, 4), "unit": "GCUPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "config": workload_config(args, extra={"cpu_sample": sample}),
+        "cpu_baseline": {"value": round(value, 4), "unit": "GCUPS", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, extra=None):
+    c = {"workload": f"wire+excitable {args.size}x{args.size} tiled_bit_planes W64, {args.ca_steps} steps each, "
+                     f"traverser autotuned (simple | temporal k)",
+         "automata": list(AUTOMATA), "x_size": args.size, "y_size": args.size, "ca_steps_per_step": args.ca_steps,
+         "layout": "tiled_bit_planes", "word_size": WORD_BITS,
+         "l2": "inputs larger than L2 (ping-pong planes 128 MiB + 192 MiB), no flush"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------- our arm
+def our_arm(args, rank: int, world: int):
+    import numpy as np
+    import torch
+    from cellato_b200 import autotune, inputs, lib
+    from cellato_b200.device import DevicePlanes
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    X = Y = args.size
+    grids = {}
+    for a in AUTOMATA:
+        r = inputs.RULE_ID[a]
+        nb = inputs.PLANES[r]
+        cells = torch.from_numpy(inputs.workload_grid(a, X, Y, SEED + rank)).to(dev)
+        pa, pb = DevicePlanes(nb, X, Y, dev), DevicePlanes(nb, X, Y, dev)
+        pa.pack_from(cells, LAYOUT, WORD_BITS, sp)
+        init = DevicePlanes(nb, X, Y, dev)
+        init.buf.copy_(pa.buf)
+        del cells
+        grids[a] = {"rule": r, "nb": nb, "a": pa, "b": pb, "init": init}
+    torch.cuda.synchronize()
+
+    # autotune per automaton (on scratch copies of the planes)
+    for a, g in grids.items():
+        choice = autotune.tune(g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, use_cache=False)
+        g["choice"] = choice
+        g["a"].buf.copy_(g["init"].buf)
+    torch.cuda.synchronize()
+
+    def launches(g):
+        c = g["choice"]
+        return args.ca_steps if c["mode"] == "simple" else -(-args.ca_steps // c["k"])
+
+    def one_step(t0, events=None):
+        for a, g in grids.items():
+            if events is not None:
+                events[a][0].record(stream)
+            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, t0,
+                                args.ca_steps, sp)
+            if in_b:
+                g["a"], g["b"] = g["b"], g["a"]
+            if events is not None:
+                events[a][1].record(stream)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    t0 = 0
+    for _ in range(args.warmup):
+        one_step(t0)
+        t0 += args.ca_steps
+    torch.cuda.synchronize()
+    barrier()
+
+    per = {a: [] for a in AUTOMATA}
+    with ClockSampler(dev.index) as clocks:
+        torch.cuda.synchronize()
+        barrier()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        step_events = []
+        for _ in range(args.steps):
+            ev = {a: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for a in AUTOMATA}
+            one_step(t0, ev)
+            step_events.append(ev)
+            t0 += args.ca_steps
+        stop.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ms = start.elapsed_time(stop)
+    for ev in step_events:
+        for a in AUTOMATA:
+            per[a].append(ev[a][0].elapsed_time(ev[a][1]))
+    ms = max_over_ranks(ms, world)
+
+    cells_per_step = len(AUTOMATA) * X * Y * args.ca_steps
+    value = cells_per_step * args.steps * world / (ms * 1e-3) / 1e9
+    per_gcups = {a: X * Y * args.ca_steps * args.steps / (sum(per[a]) * 1e-3) / 1e9 for a in AUTOMATA}
+    n_launch = sum(launches(g) for g in grids.values()) * args.steps
+
+    # ---- end to end through the C ABI with host buffers
+    host_in, host_out = {}, {}
+    for a, g in grids.items():
+        host_in[a] = [torch.empty(g["init"].plane_bytes, dtype=torch.uint8).pin_memory() for _ in range(g["nb"])]
+        host_out[a] = [torch.empty(g["init"].plane_bytes, dtype=torch.uint8).pin_memory() for _ in range(g["nb"])]
+        for p in range(g["nb"]):
+            host_in[a][p].copy_(g["init"].view(p).cpu())
+    h2d = sum(g["nb"] * g["init"].plane_bytes for g in grids.values())
+    d2h = h2d
+    L = lib.load()
+
+    def e2e_step(t0):
+        for a, g in grids.items():
+            nb, pb_ = g["nb"], g["init"].plane_bytes
+            lib.check(L.cellato_planes_upload(nb, lib.ptr_array(g["a"].ptrs),
+                                              lib.ptr_array([t.data_ptr() for t in host_in[a]]), pb_, sp))
+            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, t0,
+                                args.ca_steps, sp)
+            res = g["b"] if in_b else g["a"]
+            lib.check(L.cellato_planes_download(nb, lib.ptr_array([t.data_ptr() for t in host_out[a]]),
+                                                lib.ptr_array(res.ptrs), pb_, sp))
+
+    e2e_step(0)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step(0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    e2e_value = cells_per_step * args.steps * world / (e2e_ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel (the automaton with the most time)
+    peaks = measured_peaks()
+    dom = max(AUTOMATA, key=lambda a: sum(per[a]))
+    g = grids[dom]
+    n_dom = launches(g) * args.steps
+    avg_launch_ms = sum(per[dom]) / n_dom
+    bytes_per_launch = 2 * g["nb"] * g["init"].plane_bytes  # read + write every plane once per launch
+    achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9
+    peak = peaks["hbm_gbs"]
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None,
+            "kernel": f"{'temporal_kernel' if g['choice']['mode'] == 'temporal' else 'simple_step_kernel'} "
+                      f"({dom}, k={g['choice']['k']})",
+            "peak_source": peaks["source"],
+            "bytes_per_launch": bytes_per_launch, "avg_launch_ms": round(avg_launch_ms, 4),
+            # what the same GCUPS would need from HBM with one step per launch
+            "single_step_equivalent_frac": round(per_gcups[dom] * 1e9 * g["nb"] / 4 / 1e9 / peak, 4)}
+
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        kind, run = load_reference_cpu()
+        th = host_threads()
+        v, sample = cpu_sample(run, th, target_s=10.0)
+        v1, sample1 = cpu_sample(run, 1, target_s=5.0)
+        cpu = {"value": round(v, 4), "unit": "GCUPS", "cores": th, "kind": kind, "sample": sample,
+               "single_core": {"value": round(v1, 4), "cores": 1, "sample": sample1}}
+    line = {
+        "metric": "GCUPS", "value": round(value, 1), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded i.i.d. grids)",
+        "config": workload_config(args, extra={
+            "traverser": {a: grids[a]["choice"]["mode"] + (f" k={grids[a]['choice']['k']}"
+                                                           if grids[a]["choice"]["mode"] == "temporal" else "")
+                          for a in AUTOMATA},
+            "parallelism": f"replicas x{world}"}),
+        "per_automaton_gcups": {a: round(v, 1) for a, v in per_gcups.items()},
+        "e2e": {"value": round(e2e_value, 1), "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": n_launch,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json)"}
+    except (OSError, ValueError, KeyError):
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def max_over_ranks(ms: float, world: int) -> float:
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world)
+        else:
+            our_arm(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

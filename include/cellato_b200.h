@@ -112,6 +112,17 @@ int cellato_planes_upload(int nb, void* const* dev_planes, const void* const* ho
 int cellato_planes_download(int nb, void* const* host_planes, const void* const* dev_planes, size_t bytes,
                             cellato_stream_t stream);
 
+/* ---- device packing (replaces the host loops of the grid classes:
+ *      bit_planes_grid.hpp:234-270 pack, :97-124 get_cell; tiled
+ *      tiled_bit_planes_grid.hpp:243-288, :100-139) ------------------------ */
+
+/* cells: device array of X*Y uint8 state-dictionary indices (row-major);
+ * planes: nb device planes in the given layout.  Stream-ordered, no allocation. */
+int cellato_pack_cells(int layout, int word_bits, int nb, const uint8_t* cells, int x_cells, int y_cells,
+                       void* const* planes, cellato_stream_t stream);
+int cellato_unpack_cells(int layout, int word_bits, int nb, const void* const* planes, int x_cells, int y_cells,
+                         uint8_t* cells, cellato_stream_t stream);
+
 /* ---- traversers ----------------------------------------------------------- */
 
 /* Simple traverser (replaces include/traversers/cuda/simple.cu:43-87 with

@@ -102,3 +102,19 @@ def test_temporal_tile_too_large(cuda):
     with pytest.raises(lib.CellatoError) as e:
         lib.run_temporal("game-of-life", 0, 64, a, b, 64, 8, 0, 4, k=4, tile_rows=8 * 1000)
     assert e.value.status == lib.ESMEM
+
+
+@pytest.mark.parametrize("layout,W", LAYOUTS)
+def test_device_pack_matches_reference_layout(cuda, oracle, layout, W):
+    """cellato_pack_cells writes the reference's plane bytes; unpack inverts it."""
+    import torch
+    from cellato_b200.device import DevicePlanes
+    rng = np.random.default_rng(W + layout)
+    for nb in (1, 2, 3, 4, 5):
+        for X, Y in [(64, 8), (192, 24), (1024, 64)]:
+            cells = rng.integers(0, 1 << nb, size=(Y, X), dtype=np.uint8)
+            d = DevicePlanes(nb, X, Y)
+            d.pack_from(torch.from_numpy(cells).cuda(), layout, W)
+            torch.cuda.synchronize()
+            assert np.array_equal(d.download(), oracle.pack(layout, W, nb, cells)), (nb, X, Y)
+            assert np.array_equal(d.unpack(layout, W).cpu().numpy(), cells), (nb, X, Y)
