@@ -47,6 +47,8 @@ namespace cellato::b200 {
 
 using word = std::uint32_t;
 
+constexpr int MAX_OUT_PLANES = 8;  // planes of a stored state
+
 // ---------------------------------------------------------------- bit vectors
 template <int B>
 struct planes {
@@ -76,7 +78,7 @@ constexpr int const_width(long long v) { return v == 0 ? 1 : highest_bit(v) + 2;
 constexpr int exact_log2(long long v) { return highest_bit(v); }
 
 template <long long V>
-CB_HD planes<const_width(V)> from_constant() {
+CB_HD constexpr planes<const_width(V)> from_constant() {
     static_assert(V >= 0, "negative literals are not representable as bit planes");
     planes<const_width(V)> r;
 #pragma unroll
@@ -85,12 +87,12 @@ CB_HD planes<const_width(V)> from_constant() {
 }
 
 // A condition used as a value is a one-plane vector.
-CB_HD planes<1> as_planes(word w) { return planes<1>{{w}}; }
+CB_HD constexpr planes<1> as_planes(word w) { return planes<1>{{w}}; }
 template <int B>
-CB_HD planes<B> as_planes(planes<B> v) { return v; }
+CB_HD constexpr planes<B> as_planes(planes<B> v) { return v; }
 
 template <int N, int B>
-CB_HD planes<N> resize(planes<B> a) {
+CB_HD constexpr planes<N> resize(planes<B> a) {
     planes<N> r;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.p[i] = i < B ? a.p[i < B ? i : 0] : word(0);
@@ -99,7 +101,7 @@ CB_HD planes<N> resize(planes<B> a) {
 
 // Ripple-carry add modulo 2^max(A, B).
 template <int A, int B>
-CB_HD planes<cmax(A, B)> add(planes<A> a, planes<B> b) {
+CB_HD constexpr planes<cmax(A, B)> add(planes<A> a, planes<B> b) {
     constexpr int M = cmax(A, B), m = cmin(A, B);
     planes<M> r;
     word carry = 0;
@@ -119,7 +121,7 @@ CB_HD planes<cmax(A, B)> add(planes<A> a, planes<B> b) {
 }
 
 template <int A, int B>
-CB_HD planes<cmax(A, B)> bor(planes<A> a, planes<B> b) {
+CB_HD constexpr planes<cmax(A, B)> bor(planes<A> a, planes<B> b) {
     constexpr int M = cmax(A, B);
     planes<M> r;
 #pragma unroll
@@ -132,7 +134,7 @@ CB_HD planes<cmax(A, B)> bor(planes<A> a, planes<B> b) {
 }
 
 template <int A, int B>
-CB_HD planes<cmax(A, B)> band(planes<A> a, planes<B> b) {
+CB_HD constexpr planes<cmax(A, B)> band(planes<A> a, planes<B> b) {
     constexpr int M = cmax(A, B);
     planes<M> r;
 #pragma unroll
@@ -145,14 +147,14 @@ CB_HD planes<cmax(A, B)> band(planes<A> a, planes<B> b) {
 }
 
 template <int B>
-CB_HD planes<B> mask(planes<B> a, word m) {
+CB_HD constexpr planes<B> mask(planes<B> a, word m) {
 #pragma unroll
     for (int i = 0; i < B; ++i) a.p[i] &= m;
     return a;
 }
 
 template <int A, int B>
-CB_HD word eq(planes<A> a, planes<B> b) {
+CB_HD constexpr word eq(planes<A> a, planes<B> b) {
     word r = ~word(0);
 #pragma unroll
     for (int i = 0; i < cmax(A, B); ++i) {
@@ -164,11 +166,11 @@ CB_HD word eq(planes<A> a, planes<B> b) {
 }
 
 template <int A, int B>
-CB_HD word ne(planes<A> a, planes<B> b) { return ~eq(a, b); }
+CB_HD constexpr word ne(planes<A> a, planes<B> b) { return ~eq(a, b); }
 
 // Unsigned a > b, most significant plane first.
 template <int A, int B>
-CB_HD word gt(planes<A> a, planes<B> b) {
+CB_HD constexpr word gt(planes<A> a, planes<B> b) {
     word result = 0, decided = 0;
 #pragma unroll
     for (int i = cmax(A, B) - 1; i >= 0; --i) {
@@ -181,11 +183,11 @@ CB_HD word gt(planes<A> a, planes<B> b) {
 }
 
 template <int A, int B>
-CB_HD word lt(planes<A> a, planes<B> b) { return gt(b, a); }
+CB_HD constexpr word lt(planes<A> a, planes<B> b) { return gt(b, a); }
 
 // "all NB planes spell the constant S" -- equals_to<S> of a stored state.
 template <int S, int NB>
-CB_HD word eq_const(const word* p) {
+CB_HD constexpr word eq_const(const word* p) {
     word r = ~word(0);
 #pragma unroll
     for (int i = 0; i < NB; ++i) r &= ((S >> i) & 1) ? p[i] : ~p[i];
@@ -193,8 +195,8 @@ CB_HD word eq_const(const word* p) {
 }
 
 // Full adder / half adder on words (each output is one LOP3).
-CB_HD word xor3(word a, word b, word c) { return a ^ b ^ c; }
-CB_HD word maj3(word a, word b, word c) { return (a & b) | (c & (a ^ b)); }
+CB_HD constexpr word xor3(word a, word b, word c) { return a ^ b ^ c; }
+CB_HD constexpr word maj3(word a, word b, word c) { return (a & b) | (c & (a ^ b)); }
 
 // Funnel shifts that bring a neighbour word's edge bit in.
 // shl1(prev, cur): bit i = cur bit i-1, bit 0 = prev bit 31   (cell x-1)
@@ -380,13 +382,15 @@ CB_HD row_feat<NB, Targets> make_row_feat(const word* C, const word* L, const wo
 // the output row's global y.
 template <class RF, int TP>
 struct ctx {
+    static constexpr int tp = TP;
+    static constexpr bool symbolic = false;
     const RF& up;
     const RF& mid;
     const RF& dn;
     int ypar;
 
     template <int dy>
-    CB_HD const RF& row() const {
+    CB_HD constexpr const RF& row() const {
         if constexpr (dy < 0)
             return up;
         else if constexpr (dy > 0)
@@ -397,8 +401,8 @@ struct ctx {
     // The vertical Margolus partner of the output row is y+1 when (y + t) is
     // even and y-1 otherwise (include/evaluators/standard.hpp:183-197).  The
     // choice is made per word value (a select), never by picking a struct.
-    CB_HD bool margolus_down() const { return ((ypar ^ TP) == 0); }
-    CB_HD word pick(word down_value, word up_value) const { return margolus_down() ? down_value : up_value; }
+    CB_HD constexpr bool margolus_down() const { return ((ypar ^ TP) == 0); }
+    CB_HD constexpr word pick(word down_value, word up_value) const { return margolus_down() ? down_value : up_value; }
 };
 
 // Bits whose horizontal Margolus partner is x+1: even x on even steps, odd x
@@ -412,14 +416,37 @@ struct lower {
     static_assert(sizeof(E) == 0, "AST node not supported by the B200 lowering");
 };
 
+// Signal nodes: the leaves of a rule's state-transition logic -- neighbour
+// states, neighbourhood counts and "any neighbour is ..." tests.  Everything
+// above them is a pure per-cell boolean function (see rule_net below).
+template <class E>
+struct is_signal : std::false_type {};
+template <int dx, int dy>
+struct is_signal<ast::neighbor_at<dx, dy>> : std::true_type {};
+template <class T, class N>
+struct is_signal<ast::count_neighbors<T, N>> : std::true_type {};
+template <>
+struct is_signal<ast::margolus_180_neighbor> : std::true_type {};
+template <class T, auto Z>
+struct is_signal<ast::greater_than<ast::count_neighbors<T, ast::moore_8_neighbors>, ast::constant<Z>>>
+    : std::bool_constant<Z == 0> {};
+template <class T, auto Z>
+struct is_signal<ast::greater_than<ast::count_neighbors<T, ast::von_neumann_4_neighbors>, ast::constant<Z>>>
+    : std::bool_constant<Z == 0> {};
+
 // Evaluate node E (free function, so that node bodies can recurse by name).
+// In a symbolic context (compile-time truth-table evaluation) signal nodes
+// yield the truth-table patterns of their input variables.
 template <class Dict, class Targets, class E, class C>
-CB_HD auto ev(const C& c) {
-    return lower<Dict, Targets, E>::eval(c);
+CB_HD constexpr auto ev(const C& c) {
+    if constexpr (C::symbolic && is_signal<E>::value)
+        return c.template sig<E>();
+    else
+        return lower<Dict, Targets, E>::eval(c);
 }
 
 template <class T>
-CB_HD word as_cond(T v) {
+CB_HD constexpr word as_cond(T v) {
     if constexpr (std::is_same_v<T, word>)
         return v;
     else {
@@ -431,13 +458,13 @@ CB_HD word as_cond(T v) {
 template <class Dict, class Targets, auto V>
 struct lower<Dict, Targets, ast::constant<V>> {
     template <class C>
-    CB_HD static auto eval(const C&) { return from_constant<(long long)V>(); }
+    CB_HD static constexpr auto eval(const C&) { return from_constant<(long long)V>(); }
 };
 
 template <class Dict, class Targets, auto V>
 struct lower<Dict, Targets, ast::state_constant<V>> {
     template <class C>
-    CB_HD static auto eval(const C&) { return from_constant<(long long)Dict::state_to_index(V)>(); }
+    CB_HD static constexpr auto eval(const C&) { return from_constant<(long long)Dict::state_to_index(V)>(); }
 };
 
 template <class Dict, class Targets, int dx, int dy>
@@ -445,7 +472,7 @@ struct lower<Dict, Targets, ast::neighbor_at<dx, dy>> {
     static_assert(dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1, "neighbor_at offsets are limited to -1..1");
     static constexpr int NB = Dict::needed_bits;
     template <class C>
-    CB_HD static planes<NB> eval(const C& c) {
+    CB_HD static constexpr planes<NB> eval(const C& c) {
         planes<NB> r;
         const auto& row = c.template row<dy>();
 #pragma unroll
@@ -457,7 +484,7 @@ struct lower<Dict, Targets, ast::neighbor_at<dx, dy>> {
 template <class Dict, class Targets, class Cn, class T, class E>
 struct lower<Dict, Targets, ast::if_then_else<Cn, T, E>> {
     template <class C>
-    CB_HD static auto eval(const C& c) {
+    CB_HD static constexpr auto eval(const C& c) {
         const word m = as_cond(ev<Dict, Targets, Cn>(c));
         auto t = ev<Dict, Targets, T>(c);
         auto e = ev<Dict, Targets, E>(c);
@@ -471,7 +498,7 @@ struct lower<Dict, Targets, ast::if_then_else<Cn, T, E>> {
 template <class Dict, class Targets, class L, class R>
 struct lower<Dict, Targets, ast::and_<L, R>> {
     template <class C>
-    CB_HD static word eval(const C& c) {
+    CB_HD static constexpr word eval(const C& c) {
         return as_cond(ev<Dict, Targets, L>(c)) & as_cond(ev<Dict, Targets, R>(c));
     }
 };
@@ -479,7 +506,7 @@ struct lower<Dict, Targets, ast::and_<L, R>> {
 template <class Dict, class Targets, class L, class R>
 struct lower<Dict, Targets, ast::or_<L, R>> {
     template <class C>
-    CB_HD static word eval(const C& c) {
+    CB_HD static constexpr word eval(const C& c) {
         return as_cond(ev<Dict, Targets, L>(c)) | as_cond(ev<Dict, Targets, R>(c));
     }
 };
@@ -487,13 +514,13 @@ struct lower<Dict, Targets, ast::or_<L, R>> {
 template <class Dict, class Targets, class V>
 struct lower<Dict, Targets, ast::not_<V>> {
     template <class C>
-    CB_HD static word eval(const C& c) { return ~as_cond(ev<Dict, Targets, V>(c)); }
+    CB_HD static constexpr word eval(const C& c) { return ~as_cond(ev<Dict, Targets, V>(c)); }
 };
 
 template <class Dict, class Targets, class L, class R>
 struct lower<Dict, Targets, ast::bit_and_<L, R>> {
     template <class C>
-    CB_HD static auto eval(const C& c) {
+    CB_HD static constexpr auto eval(const C& c) {
         auto a = ev<Dict, Targets, L>(c);
         auto b = ev<Dict, Targets, R>(c);
         if constexpr (std::is_same_v<decltype(a), word> && std::is_same_v<decltype(b), word>)
@@ -506,7 +533,7 @@ struct lower<Dict, Targets, ast::bit_and_<L, R>> {
 template <class Dict, class Targets, class L, class R>
 struct lower<Dict, Targets, ast::bit_or_<L, R>> {
     template <class C>
-    CB_HD static auto eval(const C& c) {
+    CB_HD static constexpr auto eval(const C& c) {
         auto a = ev<Dict, Targets, L>(c);
         auto b = ev<Dict, Targets, R>(c);
         if constexpr (std::is_same_v<decltype(a), word> && std::is_same_v<decltype(b), word>)
@@ -519,7 +546,7 @@ struct lower<Dict, Targets, ast::bit_or_<L, R>> {
 template <class Dict, class Targets, class L, class R>
 struct lower<Dict, Targets, ast::plus<L, R>> {
     template <class C>
-    CB_HD static auto eval(const C& c) {
+    CB_HD static constexpr auto eval(const C& c) {
         return add(as_planes(ev<Dict, Targets, L>(c)), as_planes(ev<Dict, Targets, R>(c)));
     }
 };
@@ -528,7 +555,7 @@ template <class Dict, class Targets, class L, auto V>
 struct lower<Dict, Targets, ast::modulo<L, ast::constant<V>>> {
     static_assert(V > 0 && (V & (V - 1)) == 0, "only modulo by a power of two is supported");
     template <class C>
-    CB_HD static auto eval(const C& c) {
+    CB_HD static constexpr auto eval(const C& c) {
         return resize<exact_log2(V)>(as_planes(ev<Dict, Targets, L>(c)));
     }
 };
@@ -537,7 +564,7 @@ struct lower<Dict, Targets, ast::modulo<L, ast::constant<V>>> {
     template <class Dict, class Targets, class L, class R>                                \
     struct lower<Dict, Targets, ast::NODE<L, R>> {                                        \
         template <class C>                                                                \
-        CB_HD static word eval(const C& c) {                                              \
+        CB_HD static constexpr word eval(const C& c) {                                              \
             return FN(as_planes(ev<Dict, Targets, L>(c)), as_planes(ev<Dict, Targets, R>(c))); \
         }                                                                                 \
     };
@@ -550,7 +577,7 @@ CB_COMPARE(less_than, lt)
 template <class Dict, class Targets, class V, int b>
 struct lower<Dict, Targets, ast::has_bit_set<V, b>> {
     template <class C>
-    CB_HD static word eval(const C& c) {
+    CB_HD static constexpr word eval(const C& c) {
         auto v = as_planes(ev<Dict, Targets, V>(c));
         static_assert(b >= 0 && b < decltype(v)::width, "has_bit_set bit beyond the value's width");
         return v.p[b];
@@ -559,9 +586,9 @@ struct lower<Dict, Targets, ast::has_bit_set<V, b>> {
 
 template <class Dict, class Targets, class Even, class Odd>
 struct lower<Dict, Targets, ast::alternate_algorithms<Even, Odd>> {
-    template <class RF, int TP>
-    CB_HD static auto eval(const ctx<RF, TP>& c) {
-        if constexpr (TP == 0)
+    template <class C>
+    CB_HD static constexpr auto eval(const C& c) {
+        if constexpr (C::tp == 0)
             return ev<Dict, Targets, Even>(c);
         else
             return ev<Dict, Targets, Odd>(c);
@@ -574,7 +601,7 @@ template <class Dict, class Targets, auto V>
 struct lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>> {
     static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
     template <class C>
-    CB_HD static planes<4> eval(const C& c) {
+    CB_HD static constexpr planes<4> eval(const C& c) {
         const count_cache& a = c.up.cc[slot];
         const count_cache& b = c.dn.cc[slot];
         const count_cache& m = c.mid.cc[slot];
@@ -594,7 +621,7 @@ template <class Dict, class Targets, auto V>
 struct lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>> {
     static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
     template <class C>
-    CB_HD static planes<3> eval(const C& c) {
+    CB_HD static constexpr planes<3> eval(const C& c) {
         const word u = c.up.cc[slot].P[1], d = c.dn.cc[slot].P[1];
         const count_cache& m = c.mid.cc[slot];
         const word s0 = xor3(u, d, m.s2);
@@ -610,7 +637,7 @@ struct lower<Dict, Targets,
              ast::greater_than<ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>, ast::constant<Z>>> {
     static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
     template <class C>
-    CB_HD static word eval(const C& c) {
+    CB_HD static constexpr word eval(const C& c) {
         if constexpr (Z == 0) {
             const count_cache& a = c.up.cc[slot];
             const count_cache& b = c.dn.cc[slot];
@@ -629,7 +656,7 @@ struct lower<Dict, Targets,
                                ast::constant<Z>>> {
     static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
     template <class C>
-    CB_HD static word eval(const C& c) {
+    CB_HD static constexpr word eval(const C& c) {
         if constexpr (Z == 0) {
             return c.up.cc[slot].P[1] | c.dn.cc[slot].P[1] | c.mid.cc[slot].P[0] | c.mid.cc[slot].P[2];
         } else {
@@ -643,7 +670,7 @@ struct lower<Dict, Targets,
 // Counts against a target that depends on the cell itself (e.g. cyclic's
 // (state + 1) mod 32): compare each neighbour's planes with the target.
 template <int NB, class T, class RF>
-CB_HD word neighbour_eq(const RF& row, int dxi, const T& target) {
+CB_HD constexpr word neighbour_eq(const RF& row, int dxi, const T& target) {
     planes<NB> n;
 #pragma unroll
     for (int p = 0; p < NB; ++p) n.p[p] = row.sh[dxi][p];
@@ -651,7 +678,7 @@ CB_HD word neighbour_eq(const RF& row, int dxi, const T& target) {
 }
 
 template <int N>
-CB_HD planes<4> popcount8(const word (&x)[N]) {
+CB_HD constexpr planes<4> popcount8(const word (&x)[N]) {
     static_assert(N == 8);
     // carry-save tree: 4 full adders + 3 half adders
     const word a0 = xor3(x[0], x[1], x[2]), a1 = maj3(x[0], x[1], x[2]);
@@ -667,7 +694,7 @@ template <class Dict, class Targets, class T>
 struct lower<Dict, Targets, ast::count_neighbors<T, ast::moore_8_neighbors>> {
     static constexpr int NB = Dict::needed_bits;
     template <class C>
-    CB_HD static planes<4> eval(const C& c) {
+    CB_HD static constexpr planes<4> eval(const C& c) {
         const auto t = as_planes(ev<Dict, Targets, T>(c));
         const word x[8] = {neighbour_eq<NB>(c.up, 0, t),  neighbour_eq<NB>(c.up, 1, t),
                            neighbour_eq<NB>(c.up, 2, t),  neighbour_eq<NB>(c.mid, 0, t),
@@ -681,7 +708,7 @@ template <class Dict, class Targets, class T>
 struct lower<Dict, Targets, ast::count_neighbors<T, ast::von_neumann_4_neighbors>> {
     static constexpr int NB = Dict::needed_bits;
     template <class C>
-    CB_HD static planes<3> eval(const C& c) {
+    CB_HD static constexpr planes<3> eval(const C& c) {
         const auto t = as_planes(ev<Dict, Targets, T>(c));
         const word u = neighbour_eq<NB>(c.up, 1, t), d = neighbour_eq<NB>(c.dn, 1, t);
         const word l = neighbour_eq<NB>(c.mid, 0, t), r = neighbour_eq<NB>(c.mid, 2, t);
@@ -695,7 +722,7 @@ template <class Dict, class Targets, class T, auto Z>
 struct lower<Dict, Targets, ast::greater_than<ast::count_neighbors<T, ast::moore_8_neighbors>, ast::constant<Z>>> {
     static constexpr int NB = Dict::needed_bits;
     template <class C>
-    CB_HD static word eval(const C& c) {
+    CB_HD static constexpr word eval(const C& c) {
         if constexpr (Z == 0) {
             const auto t = as_planes(ev<Dict, Targets, T>(c));
             return neighbour_eq<NB>(c.up, 0, t) | neighbour_eq<NB>(c.up, 1, t) | neighbour_eq<NB>(c.up, 2, t) |
@@ -716,7 +743,7 @@ template <class Dict, class Targets, auto V>
 struct lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::margolus_alternating_neighborhood>> {
     static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
     template <class RF, int TP>
-    CB_HD static planes<3> eval(const ctx<RF, TP>& c) {
+    CB_HD static constexpr planes<3> eval(const ctx<RF, TP>& c) {
         constexpr word M = margolus_right_mask<TP>();
         const count_cache& m = c.mid.cc[slot];
         const count_cache& u = c.up.cc[slot];
@@ -736,7 +763,7 @@ template <class Dict, class Targets>
 struct lower<Dict, Targets, ast::margolus_180_neighbor> {
     static constexpr int NB = Dict::needed_bits;
     template <class RF, int TP>
-    CB_HD static planes<NB> eval(const ctx<RF, TP>& c) {
+    CB_HD static constexpr planes<NB> eval(const ctx<RF, TP>& c) {
         constexpr word M = margolus_right_mask<TP>();
         planes<NB> r;
 #pragma unroll
@@ -748,6 +775,355 @@ struct lower<Dict, Targets, ast::margolus_180_neighbor> {
         return r;
     }
 };
+
+// ------------------------------------------------ LOP3 network synthesis
+// A rule is a per-cell boolean function of its signals.  When the signals of a
+// rule add up to at most 6 input bits, the output planes are synthesised at
+// compile time into a minimal-ish LOP3 network: the rule is evaluated once,
+// symbolically, on truth-table patterns (bit m of variable j's pattern = bit j
+// of m), and each output truth table is decomposed by Shannon expansion down to
+// sub-functions of at most three variables, each one LOP3.  Sub-functions are
+// shared across outputs by truth table.
+
+template <class... Ts>
+struct tlist {
+    static constexpr int size = sizeof...(Ts);
+};
+
+template <class L, class T>
+struct tl_has;
+template <class T, class... Ts>
+struct tl_has<tlist<Ts...>, T> : std::bool_constant<(std::is_same_v<T, Ts> || ...)> {};
+
+template <class L, class T>
+struct tl_add {
+    using type = std::conditional_t<tl_has<L, T>::value, L, L>;
+};
+template <class T, class... Ts>
+struct tl_add<tlist<Ts...>, T> {
+    using type = std::conditional_t<tl_has<tlist<Ts...>, T>::value, tlist<Ts...>, tlist<Ts..., T>>;
+};
+
+template <class L, class R>
+struct tl_merge;
+template <class L>
+struct tl_merge<L, tlist<>> {
+    using type = L;
+};
+template <class L, class T, class... Ts>
+struct tl_merge<L, tlist<T, Ts...>> {
+    using type = typename tl_merge<typename tl_add<L, T>::type, tlist<Ts...>>::type;
+};
+
+// signals_of<E, TP>: the signal nodes E depends on (alternate_algorithms
+// contributes only the branch of step parity TP).
+template <class E, int TP, class = void>
+struct signals_of {
+    using type = tlist<>;
+};
+template <class E, int TP>
+struct signals_of<E, TP, std::enable_if_t<is_signal<E>::value>> {
+    using type = tlist<E>;
+};
+template <class E>
+struct is_alternation : std::false_type {};
+template <class... As>
+struct is_alternation<ast::alternate_algorithms<As...>> : std::true_type {};
+
+template <template <class...> class N, class... Ch, int TP>
+struct signals_of<N<Ch...>, TP, std::enable_if_t<!is_signal<N<Ch...>>::value && !is_alternation<N<Ch...>>::value>> {
+    template <class Acc, class... Rest>
+    struct fold {
+        using type = Acc;
+    };
+    template <class Acc, class X, class... Rest>
+    struct fold<Acc, X, Rest...> {
+        using type = typename fold<typename tl_merge<Acc, typename signals_of<X, TP>::type>::type, Rest...>::type;
+    };
+    using type = typename fold<tlist<>, Ch...>::type;
+};
+template <class Even, class Odd, int TP>
+struct signals_of<ast::alternate_algorithms<Even, Odd>, TP, void> {
+    using type = typename signals_of<std::conditional_t<TP == 0, Even, Odd>, TP>::type;
+};
+template <class V, int b, int TP>
+struct signals_of<ast::has_bit_set<V, b>, TP, void> {
+    using type = typename signals_of<V, TP>::type;
+};
+
+// Number of planes a signal contributes.
+template <class Dict, class S>
+struct signal_width {
+    static constexpr int value = Dict::needed_bits;  // neighbor_at, margolus_180_neighbor
+};
+template <class Dict, class T>
+struct signal_width<Dict, ast::count_neighbors<T, ast::moore_8_neighbors>> {
+    static constexpr int value = 4;
+};
+template <class Dict, class T>
+struct signal_width<Dict, ast::count_neighbors<T, ast::von_neumann_4_neighbors>> {
+    static constexpr int value = 3;
+};
+template <class Dict, class T>
+struct signal_width<Dict, ast::count_neighbors<T, ast::margolus_alternating_neighborhood>> {
+    static constexpr int value = 3;
+};
+template <class Dict, class T, auto Z>
+struct signal_width<Dict, ast::greater_than<ast::count_neighbors<T, ast::moore_8_neighbors>, ast::constant<Z>>> {
+    static constexpr int value = 1;
+};
+template <class Dict, class T, auto Z>
+struct signal_width<Dict, ast::greater_than<ast::count_neighbors<T, ast::von_neumann_4_neighbors>, ast::constant<Z>>> {
+    static constexpr int value = 1;
+};
+
+template <class Dict, class L>
+struct signal_layout;
+template <class Dict, class... Ss>
+struct signal_layout<Dict, tlist<Ss...>> {
+    static constexpr int total = (0 + ... + signal_width<Dict, Ss>::value);
+    template <class S>
+    static constexpr int offset() {
+        int off = 0, found = -1;
+        ((std::is_same_v<S, Ss> ? (found = found < 0 ? off : found, 0) : 0, off += signal_width<Dict, Ss>::value),
+         ...);
+        return found;
+    }
+};
+
+// Truth-table pattern of variable j (0..4) in a 32-bit word; variable 5 is
+// constant within one half of a 64-entry table.
+CB_HD constexpr word var_pattern(int j, int half) {
+    constexpr word pat[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
+    return j < 5 ? pat[j] : (half ? ~word(0) : word(0));
+}
+
+// Symbolic evaluation context: signal S yields planes of variable patterns.
+template <class Dict, class Signals, int TP, int HALF>
+struct sym_ctx {
+    static constexpr int tp = TP;
+    static constexpr bool symbolic = true;
+    template <class S>
+    constexpr auto sig() const {
+        constexpr int off = signal_layout<Dict, Signals>::template offset<S>();
+        constexpr int w = signal_width<Dict, S>::value;
+        if constexpr (w == 1 && !std::is_same_v<S, ast::neighbor_at<0, 0>> &&
+                      !std::is_same_v<S, ast::margolus_180_neighbor>) {
+            return var_pattern(off, HALF);  // a condition
+        } else {
+            planes<w> r{};
+            for (int i = 0; i < w; ++i) r.p[i] = var_pattern(off + i, HALF);
+            return r;
+        }
+    }
+};
+
+using tt_t = unsigned long long;
+
+struct lop_node {
+    int a, b, c;  // value indices: 0..n-1 inputs, n.. nodes, CONST0 / CONST1
+    int imm;      // LOP3 immediate: f(0xF0, 0xCC, 0xAA)
+};
+
+constexpr int SYNTH_MAX_NODES = 64;
+constexpr int CONST0 = -1, CONST1 = -2;
+
+struct lop_net {
+    int n = 0;       // input variables
+    int nn = 0;      // nodes
+    int nout = 0;    // outputs
+    bool ok = true;  // false: node budget exceeded
+    lop_node nodes[SYNTH_MAX_NODES] = {};
+    tt_t node_tt[SYNTH_MAX_NODES] = {};
+    int out[MAX_OUT_PLANES] = {};
+};
+
+constexpr tt_t tt_mask(int n) { return n >= 6 ? ~tt_t(0) : ((tt_t(1) << (1 << n)) - 1); }
+constexpr tt_t tt_var(int j, int n) {
+    tt_t p = 0;
+    for (int m = 0; m < (1 << n); ++m)
+        if ((m >> j) & 1) p |= tt_t(1) << m;
+    return p;
+}
+constexpr tt_t tt_cof(tt_t t, int v, int val, int n) {
+    const tt_t pv = tt_var(v, n);
+    const int sh = 1 << v;
+    if (val) {
+        const tt_t hi = t & pv;
+        return (hi | (hi >> sh)) & tt_mask(n);
+    }
+    const tt_t lo = t & ~pv & tt_mask(n);
+    return (lo | (lo << sh)) & tt_mask(n);
+}
+constexpr int tt_support(tt_t t, int n) {
+    int s = 0;
+    for (int v = 0; v < n; ++v)
+        if (tt_cof(t, v, 0, n) != tt_cof(t, v, 1, n)) s |= 1 << v;
+    return s;
+}
+constexpr int popc(int x) {
+    int c = 0;
+    for (; x; x &= x - 1) ++c;
+    return c;
+}
+
+// Estimated node count of a function (Shannon with leaves of <= 3 variables).
+constexpr int tt_cost(tt_t t, int n, int depth = 0) {
+    const tt_t m = tt_mask(n);
+    t &= m;
+    if (t == 0 || t == m) return 0;
+    const int s = tt_support(t, n);
+    if (popc(s) == 1) {
+        for (int v = 0; v < n; ++v)
+            if (s == (1 << v) && t == tt_var(v, n)) return 0;
+        return 1;
+    }
+    if (popc(s) <= 3) return 1;
+    if (depth > 4) return 99;
+    int best = 999;
+    for (int v = 0; v < n; ++v)
+        if ((s >> v) & 1) {
+            const int c = 1 + tt_cost(tt_cof(t, v, 0, n), n, depth + 1) + tt_cost(tt_cof(t, v, 1, n), n, depth + 1);
+            if (c < best) best = c;
+        }
+    return best;
+}
+
+// Truth table of a value index (input, node or constant).
+constexpr tt_t value_tt(const lop_net& net, int idx) {
+    if (idx == CONST0) return 0;
+    if (idx == CONST1) return tt_mask(net.n);
+    if (idx < net.n) return tt_var(idx, net.n);
+    return net.node_tt[idx - net.n];
+}
+
+// 8-bit LOP3 operand pattern of a value used at operand slot `slot` (0xF0,
+// 0xCC, 0xAA), or of a constant.
+constexpr int operand_pattern(int idx, int slot) {
+    if (idx == CONST0) return 0x00;
+    if (idx == CONST1) return 0xFF;
+    return slot == 0 ? 0xF0 : (slot == 1 ? 0xCC : 0xAA);
+}
+
+constexpr int add_node(lop_net& net, int a, int b, int c, int imm, tt_t t) {
+    for (int i = 0; i < net.nn; ++i)
+        if (net.node_tt[i] == t) return net.n + i;
+    if (net.nn >= SYNTH_MAX_NODES) {
+        net.ok = false;
+        return CONST0;
+    }
+    // constant operands are folded into the immediate; give them a real register
+    net.nodes[net.nn] = lop_node{a < 0 ? 0 : a, b < 0 ? 0 : b, c < 0 ? 0 : c, imm & 0xFF};
+    net.node_tt[net.nn] = t;
+    return net.n + net.nn++;
+}
+
+constexpr int emit(lop_net& net, tt_t t) {
+    const int n = net.n;
+    const tt_t m = tt_mask(n);
+    t &= m;
+    if (t == 0) return CONST0;
+    if (t == m) return CONST1;
+    for (int v = 0; v < n; ++v)
+        if (t == tt_var(v, n)) return v;
+    for (int i = 0; i < net.nn; ++i)
+        if (net.node_tt[i] == t) return n + i;
+    const int s = tt_support(t, n);
+    if (popc(s) <= 3) {
+        int vars[3] = {0, 0, 0}, k = 0;
+        for (int v = 0; v < n && k < 3; ++v)
+            if ((s >> v) & 1) vars[k++] = v;
+        int imm = 0;
+        for (int bit = 0; bit < 8; ++bit) {
+            const int xa = (bit >> 2) & 1, xb = (bit >> 1) & 1, xc = bit & 1;
+            int mt = 0;
+            if (k > 0 && xa) mt |= 1 << vars[0];
+            if (k > 1 && xb) mt |= 1 << vars[1];
+            if (k > 2 && xc) mt |= 1 << vars[2];
+            if ((t >> mt) & 1) imm |= 1 << bit;
+        }
+        return add_node(net, vars[0], vars[1], vars[2], imm, t);
+    }
+    // Shannon split on the variable with the cheapest cofactors
+    int best_v = -1, best_c = 1 << 20;
+    for (int v = 0; v < n; ++v)
+        if ((s >> v) & 1) {
+            const int c = tt_cost(tt_cof(t, v, 0, n), n) + tt_cost(tt_cof(t, v, 1, n), n);
+            if (c < best_c) best_c = c, best_v = v;
+        }
+    const int i0 = emit(net, tt_cof(t, best_v, 0, n));
+    const int i1 = emit(net, tt_cof(t, best_v, 1, n));
+    // v ? i1 : i0
+    const int pv = 0xF0, p1 = operand_pattern(i1, 1), p0 = operand_pattern(i0, 2);
+    const int imm = (pv & p1) | (~pv & p0);
+    return add_node(net, best_v, i1, i0, imm, t);
+}
+
+// The synthesised network of rule E at step parity TP (ok == false when the
+// rule has more than 6 signal bits or the node budget overflows).
+template <class Dict, class Targets, class E, int TP>
+struct synth {
+    using signals = typename signals_of<E, TP>::type;
+    using layout = signal_layout<Dict, signals>;
+    static constexpr int n = layout::total;
+    static constexpr int NB = Dict::needed_bits;
+
+    template <int HALF>
+    static constexpr auto table_half() {
+        return as_planes(ev<Dict, Targets, E>(sym_ctx<Dict, signals, TP, HALF>{}));
+    }
+
+    static constexpr lop_net build() {
+        lop_net net;
+        if (n > 6 || n < 1) {
+            net.ok = false;
+            return net;
+        }
+        net.n = n;
+        net.nout = NB;
+        constexpr auto lo = table_half<0>();
+        constexpr auto hi = table_half<1>();
+        constexpr int B = decltype(lo)::width;
+        tt_t tts[MAX_OUT_PLANES] = {};
+        for (int p = 0; p < NB; ++p) {
+            if (p >= B) {
+                tts[p] = 0;
+                continue;
+            }
+            const tt_t l = lo.p[p < B ? p : 0], h = hi.p[p < B ? p : 0];
+            tts[p] = n <= 5 ? (tt_t(l) & tt_mask(n)) : (tt_t(l) | (tt_t(h) << 32));
+        }
+        for (int p = 0; p < NB; ++p) net.out[p] = emit(net, tts[p]);
+        return net;
+    }
+    static constexpr lop_net net = build();
+    static constexpr bool ok = net.ok;
+};
+
+template <int IMM>
+CB_HD word lop3(word a, word b, word c) {
+#if defined(__CUDA_ARCH__)
+    word d;
+    asm("lop3.b32 %0, %1, %2, %3, %4;" : "=r"(d) : "r"(a), "r"(b), "r"(c), "n"(IMM));
+    return d;
+#else
+    word r = 0;
+    for (int k = 0; k < 8; ++k)
+        if ((IMM >> k) & 1) r |= (((k >> 2) & 1) ? a : ~a) & (((k >> 1) & 1) ? b : ~b) & ((k & 1) ? c : ~c);
+    return r;
+#endif
+}
+
+template <const lop_net& NET, int I>
+CB_HD void run_node(word* v) {
+    constexpr lop_node nd = NET.nodes[I];
+    v[NET.n + I] = lop3<nd.imm>(v[nd.a], v[nd.b], v[nd.c]);
+}
+
+template <const lop_net& NET, std::size_t... I>
+CB_HD void run_net(word* v, std::index_sequence<I...>) {
+    (run_node<NET, (int)I>(v), ...);
+}
 
 // ------------------------------------------------------------------ a rule
 // rule_net<Dict, Rule>: the lowered rule.  eval() returns the NB planes of
@@ -766,10 +1142,44 @@ struct rule_net {
     template <int TP>
     CB_HD static void eval(const feat& up, const feat& mid, const feat& dn, int ypar, word* out) {
         const ctx<feat, TP> c{up, mid, dn, ypar};
-        const auto r = as_planes(ev<Dict, targets, Rule>(c));
-        constexpr int B = decltype(r)::width;
+        using S = synth<Dict, targets, Rule, TP>;
+        if constexpr (S::ok) {
+            // signals through the generic lowering, then the LOP3 network
+            word v[S::net.n + S::net.nn + 1];
+            fill_signals<TP>(c, v, typename S::signals{});
+            run_net<S::net>(v, std::make_index_sequence<S::net.nn>{});
 #pragma unroll
-        for (int p = 0; p < NB; ++p) out[p] = p < B ? r.p[p < B ? p : 0] : word(0);
+            for (int p = 0; p < NB; ++p) {
+                const int idx = S::net.out[p];
+                out[p] = idx == CONST0 ? word(0) : (idx == CONST1 ? ~word(0) : v[idx < 0 ? 0 : idx]);
+            }
+        } else {
+            const auto r = as_planes(ev<Dict, targets, Rule>(c));
+            constexpr int B = decltype(r)::width;
+#pragma unroll
+            for (int p = 0; p < NB; ++p) out[p] = p < B ? r.p[p < B ? p : 0] : word(0);
+        }
+    }
+
+    // network size (0 when the rule is evaluated by the generic lowering)
+    template <int TP>
+    static constexpr int synthesized_nodes() {
+        using S = synth<Dict, targets, Rule, TP>;
+        return S::ok ? S::net.nn : -1;
+    }
+
+  private:
+    template <int TP, class C, class... Ss>
+    CB_HD static void fill_signals(const C& c, word* v, tlist<Ss...>) {
+        using L = signal_layout<Dict, tlist<Ss...>>;
+        (
+            [&] {
+                const auto s = as_planes(ev<Dict, targets, Ss>(c));
+                constexpr int off = L::template offset<Ss>();
+#pragma unroll
+                for (int i = 0; i < decltype(s)::width; ++i) v[off + i] = s.p[i];
+            }(),
+            ...);
     }
 };
 
