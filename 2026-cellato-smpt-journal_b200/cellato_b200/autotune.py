@@ -17,8 +17,9 @@ import threading
 
 from . import lib
 
-DEFAULT_CANDIDATES = (("simple", 1), ("temporal", 2), ("temporal", 4), ("temporal", 6), ("temporal", 8),
-                      ("temporal", 12), ("temporal", 16))
+DEFAULT_CANDIDATES = (("simple_register", 1), ("simple_stream", 1), ("temporal", 2),
+                      ("temporal", 4), ("temporal", 6), ("temporal", 8), ("temporal", 12), ("temporal", 16))
+_VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2}
 
 _lock = threading.Lock()
 _memo: dict = {}
@@ -62,8 +63,12 @@ def _store_file(key: str, value: dict) -> None:
 def run(choice: dict, rule: int, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int,
         steps: int, stream: int = 0) -> int:
     """Run `steps` steps with a tuned choice; returns 1 if the result is in planes_b."""
-    if choice["mode"] == "simple":
-        return lib.run_simple(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, stream)
+    if choice["mode"] in _VARIANT:
+        lib.set_simple_variant(_VARIANT[choice["mode"]])
+        try:
+            return lib.run_simple(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, stream)
+        finally:
+            lib.set_simple_variant(0)
     return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
                             choice.get("tile_rows", 0), stream)
 

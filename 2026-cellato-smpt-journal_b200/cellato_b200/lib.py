@@ -27,6 +27,7 @@ EXPORTED = [
     "cellato_planes_alloc", "cellato_planes_free", "cellato_planes_upload", "cellato_planes_download",
     "cellato_pack_cells", "cellato_unpack_cells",
     "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
+    "cellato_device_wait_timeouts", "cellato_set_simple_variant",
 ]
 
 
@@ -117,6 +118,20 @@ def pack_cells(layout: int, word_bits: int, nb: int, cells_ptr: int, X: int, Y: 
 def unpack_cells(layout: int, word_bits: int, nb: int, planes, X: int, Y: int, cells_ptr: int, stream: int = 0) -> None:
     """nb device planes -> device uint8 cells (row-major)."""
     check(load().cellato_unpack_cells(layout, word_bits, nb, ptr_array(planes), X, Y, cells_ptr, stream))
+
+
+def set_simple_variant(variant: int) -> None:
+    """0 automatic, 1 register-band kernel, 2 bulk-copy streaming kernel (linear layout)."""
+    check(load().cellato_set_simple_variant(variant))
+
+
+def device_wait_timeouts() -> int:
+    """Bounded device waits that gave up since the last call (0 when healthy)."""
+    c = ctypes.c_uint(0)
+    rc = load().cellato_device_wait_timeouts(ctypes.byref(c))
+    if rc not in (OK, ETIMEDOUT):
+        check(rc)
+    return c.value
 
 
 def run_temporal(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,

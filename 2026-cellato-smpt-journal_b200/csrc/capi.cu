@@ -214,6 +214,24 @@ int cellato_run_simple(int rule, int layout, int word_bits, void* const* planes_
     return CELLATO_OK;
 }
 
+int cellato_set_simple_variant(int variant) {
+    if (variant < 0 || variant > 2) return fail(CELLATO_EINVAL, "simple kernel variant must be 0, 1 or 2");
+    simple_variant() = variant;
+    return CELLATO_OK;
+}
+
+int cellato_device_wait_timeouts(unsigned* count) {
+    if (!count) return fail(CELLATO_EINVAL, "count must not be NULL");
+    *count = 0;
+    for (int r = 0; r < CELLATO_RULE_COUNT; ++r) {
+        unsigned c = 0;
+        cudaError_t e = ops_of(r)->take_wait_timeouts(&c);
+        if (e != cudaSuccess) return cuda_fail(e, "reading the device wait-timeout counter");
+        *count += c;
+    }
+    return *count ? fail(CELLATO_ETIMEDOUT, "%u bounded device waits gave up", *count) : CELLATO_OK;
+}
+
 int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits) {
     const rule_ops* ops = ops_of(rule);
     if (!ops) return -fail(CELLATO_EINVAL, "unknown rule id %d", rule);

@@ -151,27 +151,51 @@ __device__ __forceinline__ word from_right_lane(word v) {
     return __shfl_sync(0xffffffffu, v, (threadIdx.x + 1) & 31);
 }
 
-template <class Net, int V>
-struct row_window {
-    using feat = typename Net::feat;
-    feat f[V];
-};
-
-// Features of one row from its raw words: C[p][v] plus left/right edge words.
+// Features of one row of a lane's V words.  The predicates of the rule's count
+// targets are computed on the lane's own words and only those one-plane
+// predicates cross lanes; raw planes cross lanes only when the rule reads
+// neighbours at dx != 0.  use_l / use_r: take the left / right neighbour word
+// from Ledge / Redge (a lane at a segment edge that loaded it) instead of the
+// neighbouring lane.
 template <class Net, int NB, int V>
-__device__ __forceinline__ void build_feat(const word (&C)[NB][V], const word (&L)[NB], const word (&R)[NB],
-                                           typename Net::feat (&out)[V]) {
+__device__ __forceinline__ void row_feats(const word (&C)[NB][V], const word (&Ledge)[NB], const word (&Redge)[NB],
+                                          bool use_l, bool use_r, typename Net::feat (&out)[V]) {
+    using preds_t = typename Net::preds_t;
+    constexpr int T = Net::targets::size;
+    word col[V][NB];
 #pragma unroll
-    for (int v = 0; v < V; ++v) {
-        word c[NB], l[NB], r[NB];
+    for (int v = 0; v < V; ++v)
 #pragma unroll
-        for (int p = 0; p < NB; ++p) {
-            c[p] = C[p][v];
-            l[p] = v == 0 ? L[p] : C[p][v == 0 ? 0 : v - 1];
-            r[p] = v == V - 1 ? R[p] : C[p][v == V - 1 ? 0 : v + 1];
+        for (int p = 0; p < NB; ++p) col[v][p] = C[p][v];
+    preds_t pc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) pc[v] = Net::preds(col[v]);
+    preds_t pl = pc[0], pr = pc[0];
+    if constexpr (T > 0) {
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            pl.p[t] = from_left_lane(pc[V - 1].p[t]);
+            pr.p[t] = from_right_lane(pc[0].p[t]);
         }
-        out[v] = Net::make_feat(c, l, r);
+        if (use_l) pl = Net::preds(Ledge);
+        if (use_r) pr = Net::preds(Redge);
     }
+    word Lw[NB], Rw[NB];
+#pragma unroll
+    for (int p = 0; p < NB; ++p) {
+        if constexpr (Net::need_shift) {
+            Lw[p] = from_left_lane(C[p][V - 1]);
+            Rw[p] = from_right_lane(C[p][0]);
+            if (use_l) Lw[p] = Ledge[p];
+            if (use_r) Rw[p] = Redge[p];
+        } else {
+            Lw[p] = Rw[p] = 0;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+        out[v] = Net::make(col[v], v == 0 ? Lw : col[v == 0 ? 0 : v - 1], v == V - 1 ? Rw : col[v == V - 1 ? 0 : v + 1],
+                           pc[v], v == 0 ? pl : pc[v == 0 ? 0 : v - 1], v == V - 1 ? pr : pc[v == V - 1 ? 0 : v + 1]);
 }
 
 // ======================================================= single-step kernel
@@ -260,18 +284,8 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
             }
         }
     };
-    // neighbour words from the adjacent lanes (edge lanes keep their loads)
-    auto link_lanes = [&](const word (&raw)[BR][NB][V], word (&L)[BR][NB], word (&Rr)[BR][NB]) {
-#pragma unroll
-        for (int r = 0; r < BR; ++r)
-#pragma unroll
-            for (int p = 0; p < NB; ++p) {
-                const word l = from_left_lane(raw[r][p][V - 1]);
-                const word rr = from_right_lane(raw[r][p][0]);
-                if (seg_spans_row || lane != 0) L[r][p] = l;
-                if (seg_spans_row || lane != 31) Rr[r][p] = rr;
-            }
-    };
+    const bool use_l = !seg_spans_row && lane == 0;   // loaded, not shuffled
+    const bool use_r = !seg_spans_row && lane == 31;
     auto feat_of = [&](const word (&raw)[BR][NB][V], const word (&L)[BR][NB], const word (&Rr)[BR][NB], int r,
                        feat (&f)[V]) {
         word C[NB][V], Lw[NB], Rw[NB];
@@ -282,7 +296,7 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
             Lw[p] = L[r][p];
             Rw[p] = Rr[r][p];
         }
-        build_feat<Net, NB, V>(C, Lw, Rw, f);
+        row_feats<Net, NB, V>(C, Lw, Rw, use_l, use_r, f);
     };
 
     word cur[BR][NB][V], curL[BR][NB], curR[BR][NB];
@@ -300,28 +314,18 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
             load_lane<LAYOUT, V>(in.p[p], Xw, y, gx, rows);
 #pragma unroll
             for (int v = 0; v < V; ++v) C[p][v] = rows[0][v];
-            Lw[p] = 0;
-            Rw[p] = 0;
-            if (!seg_spans_row && (lane == 0 || lane == 31)) {
+            Lw[p] = Rw[p] = 0;
+            if (use_l || use_r) {
                 const word e = __ldg(in.p[p] + (size_t)y * Xw + (lane == 0 ? gx_left : gx_right));
-                if (lane == 0) Lw[p] = e; else Rw[p] = e;
+                if (use_l) Lw[p] = e; else Rw[p] = e;
             }
         }
-#pragma unroll
-        for (int p = 0; p < NB; ++p) {
-            const word l = from_left_lane(C[p][V - 1]);
-            const word r = from_right_lane(C[p][0]);
-            if (seg_spans_row || lane != 0) Lw[p] = l;
-            if (seg_spans_row || lane != 31) Rw[p] = r;
-        }
-        build_feat<Net, NB, V>(C, Lw, Rw, up);
+        row_feats<Net, NB, V>(C, Lw, Rw, use_l, use_r, up);
     } else {
         load_band(b0 - 1, nxt, nxtL, nxtR);
-        link_lanes(nxt, nxtL, nxtR);
         feat_of(nxt, nxtL, nxtR, BR - 1, up);
     }
     load_band(b0, cur, curL, curR);
-    link_lanes(cur, curL, curR);
     feat_of(cur, curL, curR, 0, mid);
 
     for (int b = b0; b < b1; ++b) {
@@ -332,7 +336,6 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
             if (r + 1 < BR) {
                 feat_of(cur, curL, curR, r + 1 < BR ? r + 1 : 0, dn);
             } else {
-                link_lanes(nxt, nxtL, nxtR);
                 feat_of(nxt, nxtL, nxtR, 0, dn);
             }
             const int y = b * BR + r;
@@ -388,6 +391,194 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
                 curL[r][p] = nxtL[r][p];
                 curR[r][p] = nxtR[r][p];
             }
+    }
+}
+
+// ================================================ streaming single-step kernel
+// The single-step kernel for the linear layout, fed by the bulk-copy engine.
+// Each warp owns a segment of 32*V words of every row (as above) and a ring of
+// STAGES shared-memory stages of BR rows.  Lane 0 issues, per row and plane,
+// cp.async.bulk copies of the segment and of the 16-byte blocks holding the
+// words to its left and right (wrapped on the torus), completing on the stage's
+// mbarrier; the warp computes from shared memory while the next stages land.
+// Registers hold only the three-row feature window, so occupancy stays high and
+// the bytes in flight are set by the ring, not by the register file.
+//
+// Shared row layout (words): [4 left-halo][32V segment][4 right-halo]; a
+// segment cut short by the row end places its right halo right after its last
+// word, where the first idle lane reads it.  Needs Xw % 4 == 0 (16-byte rows).
+//
+// Every mbarrier wait is bounded: a wait that gives up records the failure in
+// g_stream_wait_timeouts, drains the copies this warp still has in flight
+// (again bounded) and returns; the host reads and clears the counter through
+// the rule's status entry.
+static __device__ unsigned g_stream_wait_timeouts = 0;
+
+constexpr int STREAM_STAGES = 3;
+constexpr int STREAM_BAND = 4;
+constexpr unsigned STREAM_WAIT_LIMIT = 1u << 22;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (unsigned it = 0; it < STREAM_WAIT_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+template <int NB, int V>
+constexpr int stream_row_words() {
+    return 32 * V + 8;
+}
+
+template <int NB, int V>
+constexpr int stream_smem_per_warp() {
+    return STREAM_STAGES * STREAM_BAND * NB * stream_row_words<NB, V>() * 4 + STREAM_STAGES * 8;
+}
+
+template <class Net, int NB, int V, int TP, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, plane_set out, int Xw, int Y,
+                                                                 int rows_per_cta) {
+    constexpr int BR = STREAM_BAND, S = STREAM_STAGES, RW = stream_row_words<NB, V>();
+    using feat = typename Net::feat;
+    extern __shared__ __align__(16) word smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    word* ring = smem + (size_t)warp * (S * BR * NB * RW);
+    unsigned long long* bars =
+        reinterpret_cast<unsigned long long*>(smem + (size_t)WARPS * S * BR * NB * RW) + warp * S;
+
+    const int seg = blockIdx.x * WARPS + warp;
+    const int gx0 = seg * 32 * V;          // first word of the segment
+    if (gx0 >= Xw) return;                  // whole warp: nothing of this row range
+    const int valid = min(32 * V, Xw - gx0);
+    const int gx = gx0 + lane * V;
+    const bool owns = gx < Xw;
+    const int gl = (gx0 - 4 + Xw) % Xw;     // 16-byte block left of the segment
+    const int gr = (gx0 + valid) % Xw;      // 16-byte block right of it
+    const int y0 = blockIdx.y * rows_per_cta;
+    const int y1 = min(Y, y0 + rows_per_cta);
+    if (y0 >= y1) return;
+    const int nstream = (y1 - y0) + 2;      // rows y0-1 .. y1
+    const int nchunks = (nstream + BR - 1) / BR;
+
+    auto issue = [&](int c) {  // lane 0 only
+        const int s = c % S;
+        const int r0 = c * BR;
+        const int nr = min(BR, nstream - r0);
+        const unsigned bytes = (unsigned)(nr * NB * (valid + 8) * 4);
+        mbar_expect_tx(&bars[s], bytes);
+        int y = (y0 - 1 + r0) % Y;
+        if (y < 0) y += Y;
+        for (int r = 0; r < nr; ++r) {
+            for (int p = 0; p < NB; ++p) {
+                word* dst = ring + ((size_t)(s * BR + r) * NB + p) * RW;
+                const word* row = in.p[p] + (size_t)y * Xw;
+                bulk_g2s(dst, row + gl, 16, &bars[s]);
+                bulk_g2s(dst + 4, row + gx0, (unsigned)valid * 4, &bars[s]);
+                bulk_g2s(dst + 4 + valid, row + gr, 16, &bars[s]);
+            }
+            if (++y == Y) y = 0;
+        }
+    };
+
+    if (lane == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (lane == 0)
+        for (int c = 0; c < min(S, nchunks); ++c) issue(c);
+
+    feat up[V], mid[V], dn[V];
+    int failed_at = -1;
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c % S;
+        if (!mbar_wait_bounded(&bars[s], (unsigned)(c / S) & 1u)) {
+            failed_at = c;
+            break;
+        }
+#pragma unroll
+        for (int r = 0; r < BR; ++r) {
+            const int i = c * BR + r;  // stream row: global row y0 - 1 + i
+            if (i < nstream) {
+                word C[NB][V], Lw[NB], Rw[NB];
+#pragma unroll
+                for (int p = 0; p < NB; ++p) {
+                    const word* row = ring + ((size_t)(s * BR + r) * NB + p) * RW;
+                    if constexpr (V == 4) {
+                        const uint4 q = *reinterpret_cast<const uint4*>(row + 4 + lane * 4);
+                        C[p][0] = q.x, C[p][1] = q.y, C[p][2] = q.z, C[p][3] = q.w;
+                    } else if constexpr (V == 2) {
+                        const uint2 q = *reinterpret_cast<const uint2*>(row + 4 + lane * 2);
+                        C[p][0] = q.x, C[p][1] = q.y;
+                    } else {
+                        C[p][0] = row[4 + lane];
+                    }
+                    Lw[p] = row[3];
+                    Rw[p] = row[4 + 32 * V];
+                }
+                row_feats<Net, NB, V>(C, Lw, Rw, lane == 0, lane == 31, dn);
+                if (i >= 2) {
+                    const int y = y0 + i - 2;
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        word o[NB];
+                        Net::template eval<TP>(up[v], mid[v], dn[v], y & 1, o);
+#pragma unroll
+                        for (int p = 0; p < NB; ++p) C[p][v] = o[p];
+                    }
+                    if (owns) {
+#pragma unroll
+                        for (int p = 0; p < NB; ++p) {
+                            word rows[1][V];
+#pragma unroll
+                            for (int v = 0; v < V; ++v) rows[0][v] = C[p][v];
+                            store_lane<LAYOUT_LINEAR, V>(out.p[p], Xw, y, gx, rows);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    up[v] = mid[v];
+                    mid[v] = dn[v];
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && c + S < nchunks) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(c + S);
+        }
+    }
+    if (failed_at >= 0) {
+        if (lane == 0) atomicAdd(&g_stream_wait_timeouts, 1u);
+        // drain the copies this warp still has in flight (chunks failed_at ..
+        // failed_at + S - 1 were issued) before the CTA's shared memory is released
+        for (int c = failed_at + 1; c < min(nchunks, failed_at + S); ++c)
+            mbar_wait_bounded(&bars[c % S], (unsigned)(c / S) & 1u);
     }
 }
 
@@ -447,7 +638,7 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
     const int rw0 = warp * rows_per_warp;
     const int rw1 = rw0 + rows_per_warp;
 
-    auto read_row = [&](int r, word (&C)[NB][V], word (&L)[NB], word (&Rr)[NB]) {
+    auto read_row = [&](int r, word (&C)[NB][V]) {
 #pragma unroll
         for (int p = 0; p < NB; ++p) {
             if constexpr (V % 4 == 0) {
@@ -466,12 +657,12 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
 #pragma unroll
                 for (int v = 0; v < V; ++v) C[p][v] = at(p, r, lane * V + v);
             }
-            L[p] = from_left_lane(C[p][V - 1]);
-            Rr[p] = from_right_lane(C[p][0]);
-            if (lane == 0) L[p] = 0;   // beyond the tile: its halo absorbs the error
-            if (lane == 31) Rr[p] = 0;
         }
     };
+    // Lanes 0 and 31 take their outer neighbour from the opposite end of the
+    // warp: those words sit in the 1-word halo, whose values do not matter.
+    const word no_edge[NB] = {};
+    auto feats = [&](const word (&C)[NB][V], feat (&f)[V]) { row_feats<Net, NB, V>(C, no_edge, no_edge, false, false, f); };
 
     auto write_row = [&](int r, const word (&o)[NB][V]) {
 #pragma unroll
@@ -495,14 +686,14 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
     // One output row r: dn features from row r+1 (or the saved bottom row),
     // evaluation, in-place write.  fu/fm/fd rotate roles between calls.
     auto row_body = [&](int r, int hi, int gy, const feat (&fu)[V], const feat (&fm)[V], feat (&fd)[V],
-                        const word (&botC)[NB][V], const word (&botL)[NB], const word (&botR)[NB], auto tp_tag) {
+                        const word (&botC)[NB][V], auto tp_tag) {
         constexpr int TP = decltype(tp_tag)::value;
         if (r + 1 < hi) {
-            word C[NB][V], L[NB], Rr[NB];
-            read_row(r + 1, C, L, Rr);
-            build_feat<Net, NB, V>(C, L, Rr, fd);
+            word C[NB][V];
+            read_row(r + 1, C);
+            feats(C, fd);
         } else {
-            build_feat<Net, NB, V>(botC, botL, botR, fd);
+            feats(botC, fd);
         }
         word o[NB][V];
 #pragma unroll
@@ -518,19 +709,19 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
     auto step = [&](int t, auto tp_tag) {
         const int lo = max(rw0, t);
         const int hi = min(rw1, TH - t);
-        word topC[NB][V], topL[NB], topR[NB], botC[NB][V], botL[NB], botR[NB];
+        word topC[NB][V], botC[NB][V];
         if (lo < hi) {
-            read_row(lo - 1, topC, topL, topR);
-            read_row(hi, botC, botL, botR);
+            read_row(lo - 1, topC);
+            read_row(hi, botC);
         }
         __syncthreads();
         if (lo < hi) {
             feat fa[V], fb[V], fc[V];
-            build_feat<Net, NB, V>(topC, topL, topR, fa);
+            feats(topC, fa);
             {
-                word C[NB][V], L[NB], Rr[NB];
-                read_row(lo, C, L, Rr);
-                build_feat<Net, NB, V>(C, L, Rr, fb);
+                word C[NB][V];
+                read_row(lo, C);
+                feats(C, fb);
             }
             // global row of tile row lo, advanced incrementally (no division per row)
             int gy = (y0 - HY + lo) % Y;
@@ -539,17 +730,17 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
             int r = lo;
             // three rows per trip: the feature buffers rotate by name, not by copy
             for (; r + 3 <= hi; r += 3) {
-                row_body(r, hi, gy, fa, fb, fc, botC, botL, botR, tp_tag);
+                row_body(r, hi, gy, fa, fb, fc, botC, tp_tag);
                 gy = next_gy(gy);
-                row_body(r + 1, hi, gy, fb, fc, fa, botC, botL, botR, tp_tag);
+                row_body(r + 1, hi, gy, fb, fc, fa, botC, tp_tag);
                 gy = next_gy(gy);
-                row_body(r + 2, hi, gy, fc, fa, fb, botC, botL, botR, tp_tag);
+                row_body(r + 2, hi, gy, fc, fa, fb, botC, tp_tag);
                 gy = next_gy(gy);
             }
             if (r < hi) {
-                row_body(r, hi, gy, fa, fb, fc, botC, botL, botR, tp_tag);
+                row_body(r, hi, gy, fa, fb, fc, botC, tp_tag);
                 gy = next_gy(gy);
-                if (r + 1 < hi) row_body(r + 1, hi, gy, fb, fc, fa, botC, botL, botR, tp_tag);
+                if (r + 1 < hi) row_body(r + 1, hi, gy, fb, fc, fa, botC, tp_tag);
             }
         }
         __syncthreads();

@@ -15,6 +15,13 @@
 
 namespace cellato::b200 {
 
+// Single-step kernel for the linear layout: 0 = the library's choice, 1 = the
+// register-band kernel, 2 = the bulk-copy streaming kernel.  Process-wide.
+inline int& simple_variant() {
+    static int v = 0;
+    return v;
+}
+
 struct rule_ops {
     const char* name;
     int planes;  // needed_bits
@@ -27,6 +34,8 @@ struct rule_ops {
                             int TH, int HY, cudaStream_t s);
     int temporal_words_per_lane;  // V of the temporal tile (tile width 32*V words)
     int temporal_warps;
+    // reads and clears the count of bounded waits that gave up (device-side)
+    cudaError_t (*take_wait_timeouts)(unsigned* count);
 };
 
 // Words per lane of the single-step kernel: as wide as registers allow.  A row
@@ -68,9 +77,45 @@ struct rule_kernels {
         return cudaGetLastError();
     }
 
+    // linear layout, 16-byte rows: the bulk-copy streaming kernel
+    static constexpr int STREAM_V = NB <= 2 ? 4 : 2;
+    static constexpr int STREAM_WARPS = 4;
+    static cudaError_t simple_stream(const plane_set& in, const plane_set& out, int Xw, int Y, int t,
+                                     cudaStream_t s) {
+        constexpr int V = STREAM_V;
+        const int segments = (Xw + 32 * V - 1) / (32 * V);
+        const int cta_x = (segments + STREAM_WARPS - 1) / STREAM_WARPS;
+        const long long want = 148LL * 32;
+        const int rows = (int)std::max(16LL, std::min<long long>(512, (long long)segments * Y / want));
+        const dim3 grid(cta_x, (Y + rows - 1) / rows), block(STREAM_WARPS * 32);
+        const size_t smem = (size_t)STREAM_WARPS * stream_smem_per_warp<NB, V>();
+        auto k0 = stream_step_kernel<net, NB, V, 0, STREAM_WARPS>;
+        auto k1 = stream_step_kernel<net, NB, V, 1, STREAM_WARPS>;
+        auto kern = (t & 1) ? k1 : k0;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, block, smem, s>>>(in, out, Xw, Y, rows);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t take_wait_timeouts(unsigned* count) {
+        unsigned zero = 0;
+        cudaError_t e = cudaMemcpyFromSymbol(count, g_stream_wait_timeouts, sizeof(unsigned));
+        if (e != cudaSuccess) return e;
+        return cudaMemcpyToSymbol(g_stream_wait_timeouts, &zero, sizeof(unsigned));
+    }
+
     template <int LAYOUT>
     static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t,
                                      cudaStream_t s) {
+        if constexpr (LAYOUT == LAYOUT_LINEAR) {
+            const int variant = simple_variant();
+            const bool stream_ok = Xw % 4 == 0;
+            // default: streaming for rules with three or more planes, whose
+            // register bands would otherwise cap occupancy
+            const bool use_stream = stream_ok && (variant == 2 || (variant == 0 && NB >= 2));
+            if (use_stream) return simple_stream(in, out, Xw, Y, t, s);
+        }
         constexpr int VMAX = simple_words_per_lane<net, NB, LAYOUT>();
         if constexpr (VMAX >= 4)
             if (Xw % 4 == 0) return simple_v<LAYOUT, 4>(in, out, Xw, Y, t, s);
@@ -114,7 +159,8 @@ struct rule_kernels {
     }
 
     static rule_ops ops() {
-        return rule_ops{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS};
+        return rule_ops{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS,
+                        &take_wait_timeouts};
     }
 };
 

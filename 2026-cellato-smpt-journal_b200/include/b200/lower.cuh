@@ -325,6 +325,64 @@ CB_BINARY_TARGETS(less_than)
 template <class Dict, class E>
 using targets_of = typename idedup<typename count_targets<Dict, E>::type>::type;
 
+// ------------------------------------------------- which features a rule reads
+// uses_shift<E>: E reads neighbour planes at dx != 0 (the row's planes shifted
+// by one cell); uses_sums<E>: E reads full Moore / von Neumann counts of a fixed
+// state (the per-row partial sums).  Only these features are computed.
+template <class E>
+struct is_state_const : std::false_type {};
+template <auto V>
+struct is_state_const<ast::state_constant<V>> : std::true_type {};
+
+template <class E>
+struct is_count : std::false_type {};
+template <class T, class N>
+struct is_count<ast::count_neighbors<T, N>> : std::true_type {};
+
+template <class E>
+struct is_count_test : std::false_type {};  // greater_than<count_neighbors<T, moore | von Neumann>, constant<Z>>
+template <class T, auto Z>
+struct is_count_test<ast::greater_than<ast::count_neighbors<T, ast::moore_8_neighbors>, ast::constant<Z>>>
+    : std::true_type {};
+template <class T, auto Z>
+struct is_count_test<ast::greater_than<ast::count_neighbors<T, ast::von_neumann_4_neighbors>, ast::constant<Z>>>
+    : std::true_type {};
+
+template <class E, class = void>
+struct uses_shift : std::false_type {};
+template <class E, class = void>
+struct uses_sums : std::false_type {};
+
+template <int dx, int dy>
+struct uses_shift<ast::neighbor_at<dx, dy>, void> : std::bool_constant<dx != 0> {};
+template <>
+struct uses_shift<ast::margolus_180_neighbor, void> : std::true_type {};
+template <class T, class N>
+struct uses_shift<ast::count_neighbors<T, N>, void> : std::bool_constant<!is_state_const<T>::value> {};
+template <class V, int b>
+struct uses_shift<ast::has_bit_set<V, b>, void> : uses_shift<V> {};
+template <template <class...> class N, class... Ch>
+struct uses_shift<N<Ch...>, std::enable_if_t<!is_count<N<Ch...>>::value>>
+    : std::bool_constant<(uses_shift<Ch>::value || ...)> {};
+
+template <class T, class N>
+struct uses_sums<ast::count_neighbors<T, N>, void>
+    : std::bool_constant<(is_state_const<T>::value && (std::is_same_v<N, ast::moore_8_neighbors> ||
+                                                        std::is_same_v<N, ast::von_neumann_4_neighbors>)) ||
+                         uses_sums<T>::value> {};
+template <class V, int b>
+struct uses_sums<ast::has_bit_set<V, b>, void> : uses_sums<V> {};
+template <template <class...> class N, class... Ch>
+struct uses_sums<N<Ch...>, std::enable_if_t<!is_count<N<Ch...>>::value && !is_count_test<N<Ch...>>::value>>
+    : std::bool_constant<(uses_sums<Ch>::value || ...)> {};
+// "count > 0" reads the predicates only (the OR fast path below)
+template <class T, auto Z>
+struct uses_sums<ast::greater_than<ast::count_neighbors<T, ast::moore_8_neighbors>, ast::constant<Z>>, void>
+    : std::bool_constant<Z != 0 || uses_sums<T>::value> {};
+template <class T, auto Z>
+struct uses_sums<ast::greater_than<ast::count_neighbors<T, ast::von_neumann_4_neighbors>, ast::constant<Z>>, void>
+    : std::bool_constant<Z != 0 || uses_sums<T>::value> {};
+
 // ------------------------------------------------------------ per-row cache
 // Predicate "cell == S" at dx = -1, 0, +1 and its partial sums.
 struct count_cache {
@@ -339,42 +397,50 @@ struct row_feat {
     count_cache cc[Targets::size > 0 ? Targets::size : 1];
 };
 
-// Builds a row's features from its own word (C), the word to its left (L) and
-// the word to its right (R), all NB planes.  Only bit 31 of L and bit 0 of R
-// matter.
-template <int NB, class Targets, int... S>
-CB_HD row_feat<NB, Targets> make_row_feat_impl(const word* C, const word* L, const word* R, ilist<S...>) {
+// Predicates "cell == S" of one word for every count target S.
+template <class Targets>
+struct pred_set {
+    word p[Targets::size > 0 ? Targets::size : 1];
+};
+
+template <int NB, int... S>
+CB_HD pred_set<ilist<S...>> preds_of_impl(const word* C, ilist<S...>) {
+    pred_set<ilist<S...>> r{};
+    int k = 0;
+    ((r.p[k++] = eq_const<S, NB>(C)), ...);
+    (void)k;
+    return r;
+}
+
+// Builds a row's features for one word from its own planes (C), the words to
+// its left and right (L, R: only bit 31 / bit 0 matter, read only when SHIFT)
+// and the count-target predicates of the three words.
+template <int NB, class Targets, bool SHIFT, bool SUMS>
+CB_HD row_feat<NB, Targets> make_row_feat(const word* C, const word* L, const word* R, const pred_set<Targets>& pc,
+                                          const pred_set<Targets>& pl, const pred_set<Targets>& pr) {
     row_feat<NB, Targets> f;
 #pragma unroll
     for (int p = 0; p < NB; ++p) {
-        f.sh[0][p] = shl1(L[p], C[p]);
         f.sh[1][p] = C[p];
-        f.sh[2][p] = shr1(C[p], R[p]);
+        if constexpr (SHIFT) {
+            f.sh[0][p] = shl1(L[p], C[p]);
+            f.sh[2][p] = shr1(C[p], R[p]);
+        }
     }
-    int k = 0;
-    (
-        [&] {
-            // predicate first, shift second: one predicate per word instead of three
-            const word pc = eq_const<S, NB>(C);
-            const word pl = eq_const<S, NB>(L);
-            const word pr = eq_const<S, NB>(R);
-            count_cache& c = f.cc[k++];
-            c.P[0] = shl1(pl, pc);
-            c.P[1] = pc;
-            c.P[2] = shr1(pc, pr);
+#pragma unroll
+    for (int k = 0; k < Targets::size; ++k) {
+        count_cache& c = f.cc[k];
+        c.P[0] = shl1(pl.p[k], pc.p[k]);  // predicate first, shift second
+        c.P[1] = pc.p[k];
+        c.P[2] = shr1(pc.p[k], pr.p[k]);
+        if constexpr (SUMS) {
             c.s3 = xor3(c.P[0], c.P[1], c.P[2]);
             c.c3 = maj3(c.P[0], c.P[1], c.P[2]);
             c.s2 = c.P[0] ^ c.P[2];
             c.c2 = c.P[0] & c.P[2];
-        }(),
-        ...);
-    (void)k;
+        }
+    }
     return f;
-}
-
-template <int NB, class Targets>
-CB_HD row_feat<NB, Targets> make_row_feat(const word* C, const word* L, const word* R) {
-    return make_row_feat_impl<NB, Targets>(C, L, R, Targets{});
 }
 
 // Evaluation context of one output word.  TP is the parity of the time step
@@ -1134,9 +1200,21 @@ struct rule_net {
     static constexpr int NB = Dict::needed_bits;
     using targets = targets_of<Dict, Rule>;
     using feat = row_feat<NB, targets>;
+    using preds_t = pred_set<targets>;
+    static constexpr bool need_shift = uses_shift<Rule>::value;
+    static constexpr bool need_sums = uses_sums<Rule>::value;
 
+    CB_HD static preds_t preds(const word* C) { return preds_of_impl<NB>(C, targets{}); }
+
+    // features of one word given its neighbours' predicates
+    CB_HD static feat make(const word* C, const word* L, const word* R, const preds_t& pc, const preds_t& pl,
+                           const preds_t& pr) {
+        return make_row_feat<NB, targets, need_shift, need_sums>(C, L, R, pc, pl, pr);
+    }
+
+    // features of one word from its own and its two neighbour words
     CB_HD static feat make_feat(const word* C, const word* L, const word* R) {
-        return make_row_feat<NB, targets>(C, L, R);
+        return make(C, L, R, preds(C), preds(L), preds(R));
     }
 
     template <int TP>
@@ -1148,11 +1226,7 @@ struct rule_net {
             word v[S::net.n + S::net.nn + 1];
             fill_signals<TP>(c, v, typename S::signals{});
             run_net<S::net>(v, std::make_index_sequence<S::net.nn>{});
-#pragma unroll
-            for (int p = 0; p < NB; ++p) {
-                const int idx = S::net.out[p];
-                out[p] = idx == CONST0 ? word(0) : (idx == CONST1 ? ~word(0) : v[idx < 0 ? 0 : idx]);
-            }
+            store_outputs<S::net>(v, out, std::make_index_sequence<NB>{});
         } else {
             const auto r = as_planes(ev<Dict, targets, Rule>(c));
             constexpr int B = decltype(r)::width;
@@ -1169,6 +1243,21 @@ struct rule_net {
     }
 
   private:
+    template <const lop_net& NET, std::size_t... P>
+    CB_HD static void store_outputs(const word* v, word* out, std::index_sequence<P...>) {
+        (
+            [&] {
+                constexpr int idx = NET.out[P];
+                if constexpr (idx == CONST0)
+                    out[P] = 0;
+                else if constexpr (idx == CONST1)
+                    out[P] = ~word(0);
+                else
+                    out[P] = v[idx];
+            }(),
+            ...);
+    }
+
     template <int TP, class C, class... Ss>
     CB_HD static void fill_signals(const C& c, word* v, tlist<Ss...>) {
         using L = signal_layout<Dict, tlist<Ss...>>;

@@ -238,7 +238,7 @@ def our_arm(args, rank: int, world: int):
 
     def launches(g):
         c = g["choice"]
-        return args.ca_steps if c["mode"] == "simple" else -(-args.ca_steps // c["k"])
+        return args.ca_steps if c["mode"].startswith("simple") else -(-args.ca_steps // c["k"])
 
     def one_step(t0, events=None):
         for a, g in grids.items():
@@ -334,7 +334,7 @@ def our_arm(args, rank: int, world: int):
     peak = peaks["hbm_gbs"]
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": None,
-            "kernel": f"{'temporal_kernel' if g['choice']['mode'] == 'temporal' else 'simple_step_kernel'} "
+            "kernel": f"{'temporal_kernel' if g['choice']['mode'] == 'temporal' else g['choice']['mode']} "
                       f"({dom}, k={g['choice']['k']})",
             "peak_source": peaks["source"],
             "bytes_per_launch": bytes_per_launch, "avg_launch_ms": round(avg_launch_ms, 4),

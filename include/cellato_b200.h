@@ -144,6 +144,19 @@ int cellato_run_temporal(int rule, int layout, int word_bits, void* const* plane
                          int x_cells, int y_cells, int t0, int steps, int k, int tile_rows,
                          cellato_stream_t stream, int* result_in_b);
 
+/* Selects the single-step kernel used for the linear layout: 0 = automatic,
+ * 1 = register-band kernel, 2 = bulk-copy streaming kernel (rows of 16-byte
+ * multiples only; others fall back to 1).  Process-wide, not synchronised with
+ * concurrent launches; the autotuner sweeps it.  No counterpart in the
+ * reference (one simple kernel). */
+int cellato_set_simple_variant(int variant);
+
+/* Reads and clears the number of bounded device-side waits (mbarrier waits of
+ * the streaming single-step kernel) that gave up since the last call; returns
+ * CELLATO_ETIMEDOUT when it is non-zero.  Synchronises the device.  No
+ * counterpart in the reference, whose kernels never wait. */
+int cellato_device_wait_timeouts(unsigned* count);
+
 /* Largest tile_rows the temporal kernel accepts for (rule, layout, word_bits)
  * on the current device, or a negative status. */
 int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits);

@@ -118,3 +118,18 @@ def test_device_pack_matches_reference_layout(cuda, oracle, layout, W):
             torch.cuda.synchronize()
             assert np.array_equal(d.download(), oracle.pack(layout, W, nb, cells)), (nb, X, Y)
             assert np.array_equal(d.unpack(layout, W).cpu().numpy(), cells), (nb, X, Y)
+
+
+def test_streaming_kernel_shapes_and_no_wait_timeouts(cuda, oracle):
+    """The bulk-copy streaming kernel (linear rows of 16-byte multiples):
+    segments shorter than a warp, partial last segments, wrapped halos, tall
+    and one-row grids; afterwards no bounded device wait may have given up."""
+    rng = np.random.default_rng(21)
+    for r in range(10):
+        for X, Y in [(128, 1), (128, 5), (256, 17), (384, 9), (4096 + 128, 13), (8192, 33)]:
+            cells = rng.integers(0, inputs.STATES[r], size=(Y, X), dtype=np.uint8)
+            want = oracle.run(r, cells, 5, t0=3)
+            for W in (32, 64):
+                got = run_gpu(oracle, r, 0, W, cells, 5, t0=3)
+                assert np.array_equal(got, want), (RULES[r], X, Y, W)
+    assert lib.device_wait_timeouts() == 0
