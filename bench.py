@@ -42,6 +42,13 @@ WORD_BITS = 64
 SEED = 42
 CPU_SAMPLE_SIZE = 2048
 
+# DRAM bytes (read + write) per launch measured by one ncu capture of the same
+# configuration (summaries in profiles/); keyed by (rule, mode, k, size).
+MEASURED_TRAFFIC = {
+    ("wire", "temporal", 8, 16384): (83.40e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md"),
+    ("excitable", "temporal", 16, 16384): (152.92e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -144,13 +151,18 @@ def cpu_sample(run, threads: int, target_s: float):
     grids = {a: inputs.workload_grid(a, n, n, SEED) for a in AUTOMATA}
     t = time.perf_counter()
     for a in AUTOMATA:
-        run(inputs.RULE_ID[a], grids[a], 4, threads)
+        run(inputs.RULE_ID[a], grids[a], 8, threads)
     probe = time.perf_counter() - t
-    steps = max(4, int(4 * target_s / max(probe, 1e-3)))
-    t = time.perf_counter()
-    for a in AUTOMATA:
-        run(inputs.RULE_ID[a], grids[a], steps, threads)
-    dt = time.perf_counter() - t
+    steps = max(8, int(8 * 0.5 * target_s / max(probe, 1e-3)))
+    # repeat bursts until the sample holds at least target_s of CPU work
+    dt, total_steps = 0.0, 0
+    while dt < target_s:
+        t = time.perf_counter()
+        for a in AUTOMATA:
+            run(inputs.RULE_ID[a], grids[a], steps, threads)
+        dt += time.perf_counter() - t
+        total_steps += steps
+    steps = total_steps
     cells = len(AUTOMATA) * n * n * steps
     return cells / dt / 1e9, f"{'+'.join(AUTOMATA)} {n}x{n} crops, {steps} steps each, {dt:.1f} s"
 
@@ -332,8 +344,10 @@ def our_arm(args, rank: int, world: int):
     bytes_per_launch = 2 * g["nb"] * g["init"].plane_bytes  # read + write every plane once per launch
     achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9
     peak = peaks["hbm_gbs"]
+    measured = MEASURED_TRAFFIC.get((dom, g["choice"]["mode"], g["choice"]["k"], args.size))
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": None,
+            "frac": round(achieved / peak, 4), "traffic": measured[0] if measured else None,
+            "traffic_source": measured[1] if measured else "no capture of this configuration",
             "kernel": f"{'temporal_kernel' if g['choice']['mode'] == 'temporal' else g['choice']['mode']} "
                       f"({dom}, k={g['choice']['k']})",
             "peak_source": peaks["source"],
@@ -348,7 +362,7 @@ def our_arm(args, rank: int, world: int):
         kind, run = load_reference_cpu()
         th = host_threads()
         v, sample = cpu_sample(run, th, target_s=10.0)
-        v1, sample1 = cpu_sample(run, 1, target_s=5.0)
+        v1, sample1 = cpu_sample(run, 1, target_s=10.0)
         cpu = {"value": round(v, 4), "unit": "GCUPS", "cores": th, "kind": kind, "sample": sample,
                "single_core": {"value": round(v1, 4), "cores": 1, "sample": sample1}}
     line = {
