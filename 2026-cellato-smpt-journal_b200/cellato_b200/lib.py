@@ -28,6 +28,8 @@ EXPORTED = [
     "cellato_pack_cells", "cellato_unpack_cells",
     "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
     "cellato_device_wait_timeouts", "cellato_set_simple_variant",
+    "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
+    "cellato_batch_destroy",
 ]
 
 
@@ -35,6 +37,11 @@ class CellatoError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
         self.status = status
+
+
+class BatchGrid(ctypes.Structure):
+    _fields_ = [("rule", ctypes.c_int), ("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int),
+                ("steps", ctypes.c_int), ("planes_a", ctypes.c_void_p * 8), ("planes_b", ctypes.c_void_p * 8)]
 
 
 _lib = None
@@ -62,6 +69,12 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     i = ctypes.c_int
     lib.cellato_run_simple.argtypes = [i, i, i, _PP, _PP, i, i, i, i, _vp, ctypes.POINTER(i)]
     lib.cellato_run_temporal.argtypes = [i, i, i, _PP, _PP, i, i, i, i, i, i, _vp, ctypes.POINTER(i)]
+    lib.cellato_batch_create.argtypes = [i, i, ctypes.POINTER(BatchGrid), i, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_void_p)]
+    lib.cellato_batch_launch.argtypes = [_vp, _vp]
+    lib.cellato_batch_result_in_b.argtypes = [_vp, i, ctypes.POINTER(i)]
+    lib.cellato_batch_info.argtypes = [_vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]
+    lib.cellato_batch_destroy.argtypes = [_vp]
     lib.cellato_pack_cells.argtypes = [i, i, i, _vp, i, i, _PP, _vp]
     lib.cellato_unpack_cells.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
     _lib = lib

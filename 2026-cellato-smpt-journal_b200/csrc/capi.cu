@@ -9,7 +9,7 @@
 #include <string>
 
 #include "cellato_b200.h"
-#include "rule_kernels.cuh"
+#include "capi_internal.hpp"
 
 namespace cellato::b200 {
 extern const rule_ops rule_ops_0, rule_ops_1, rule_ops_2, rule_ops_3, rule_ops_4, rule_ops_5, rule_ops_6,
@@ -18,7 +18,7 @@ extern const rule_ops rule_ops_0, rule_ops_1, rule_ops_2, rule_ops_3, rule_ops_4
 
 using namespace cellato::b200;
 
-namespace {
+namespace cellato::b200::capi {
 
 thread_local std::string g_last_error;
 
@@ -99,7 +99,9 @@ int default_tile_rows(const rule_ops* ops, int R) {
     return rows;
 }
 
-}  // namespace
+}  // namespace cellato::b200::capi
+
+using namespace cellato::b200::capi;
 
 extern "C" {
 

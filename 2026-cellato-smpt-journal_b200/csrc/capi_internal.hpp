@@ -1,0 +1,20 @@
+// Helpers shared by the C ABI translation units (capi.cu, batch.cu).
+#ifndef CELLATO_B200_CAPI_INTERNAL_HPP
+#define CELLATO_B200_CAPI_INTERNAL_HPP
+
+#include <cuda_runtime.h>
+
+#include "rule_kernels.cuh"
+
+namespace cellato::b200::capi {
+int fail(int status, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+const rule_ops* ops_of(int rule);
+int internal_layout(int layout, int word_bits);
+int band_height(int layout, int word_bits);
+int check_dims(int layout, int word_bits, int X, int Y);
+int make_sets(const rule_ops* ops, void* const* a, void* const* b, plane_set& pa, plane_set& pb);
+int default_tile_rows(const rule_ops* ops, int R);
+}  // namespace cellato::b200::capi
+
+#endif

@@ -598,8 +598,8 @@ __global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, p
 // first barrier of the step and every write happens after it.  At step t only
 // rows t .. TH-1-t are computed (the valid region shrinks by one row per step).
 template <class Net, int NB, int LAYOUT, int V, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plane_set out, int Xw, int Y, int t0,
-                                                              int k, int TH, int HY) {
+__device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
+                                              int TH, int HY, int bx, int by) {
     constexpr int R = band_rows<LAYOUT>();
     constexpr int TW = 32 * V;  // tile width in words
     using feat = typename Net::feat;
@@ -609,8 +609,8 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
     const int warp = threadIdx.x >> 5;
     const int effW = TW - 2;
     const int effH = TH - 2 * HY;
-    const int x0 = blockIdx.x * effW;  // first output word
-    const int y0 = blockIdx.y * effH;  // first output row
+    const int x0 = bx * effW;  // first output word
+    const int y0 = by * effH;  // first output row
     const int Yb = Y / R;
 
     auto at = [&](int p, int r, int s) -> word& { return tile[((size_t)p * TH + r) * TW + s]; };
@@ -770,6 +770,40 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
                 store_word_rows<LAYOUT>(out.p[p], Xw, gy0 / R, gx, rows);
             }
         }
+    }
+}
+
+template <class Net, int NB, int LAYOUT, int V, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plane_set out, int Xw, int Y, int t0,
+                                                              int k, int TH, int HY) {
+    temporal_tile<Net, NB, LAYOUT, V, WARPS>(in, out, Xw, Y, t0, k, TH, HY, blockIdx.x, blockIdx.y);
+}
+
+// ======================================================= batched temporal kernel
+// Many independent grids of one rule in one launch: persistent CTAs stride over
+// a device work list of (grid, tile, steps) items and run the temporal tile of
+// each item.  Every grid has its own planes (p[0] = a, p[1] = b), sizes and
+// step budget; all items of a launch start at the same global step t0 and use
+// the launch's halo HY, which covers their step count (steps <= k).
+struct batch_grid_desc {
+    plane_set p[2];
+    int Xw, Y;
+};
+
+struct batch_item {
+    int grid, tx, ty, steps;
+};
+
+template <class Net, int NB, int LAYOUT, int V, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) temporal_batch_kernel(const batch_grid_desc* __restrict__ grids,
+                                                                    const batch_item* __restrict__ items, int n_items,
+                                                                    int parity, int t0, int TH, int HY) {
+    for (int i = blockIdx.x; i < n_items; i += gridDim.x) {
+        const batch_item it = items[i];
+        const batch_grid_desc& g = grids[it.grid];
+        temporal_tile<Net, NB, LAYOUT, V, WARPS>(g.p[parity], g.p[parity ^ 1], g.Xw, g.Y, t0, it.steps, TH, HY, it.tx,
+                                                  it.ty);
+        __syncthreads();  // the next item reloads the tile
     }
 }
 

@@ -36,6 +36,11 @@ struct rule_ops {
     int temporal_warps;
     // reads and clears the count of bounded waits that gave up (device-side)
     cudaError_t (*take_wait_timeouts)(unsigned* count);
+    // batched temporal launch over a work list (see temporal_batch_kernel);
+    // prepare_batch sets the kernel's shared-memory limit (call outside capture)
+    cudaError_t (*prepare_batch)(int layout, int TH);
+    cudaError_t (*temporal_batch)(int layout, const batch_grid_desc* grids, const batch_item* items, int n_items,
+                                  int parity, int t0, int TH, int HY, int ctas, cudaStream_t s);
 };
 
 // Words per lane of the single-step kernel: as wide as registers allow.  A row
@@ -158,9 +163,48 @@ struct rule_kernels {
         return cudaErrorInvalidValue;
     }
 
+    template <int LAYOUT>
+    static auto batch_kernel() {
+        return temporal_batch_kernel<net, NB, LAYOUT, TEMPORAL_V, TEMPORAL_WARPS>;
+    }
+    static size_t tile_smem(int TH) { return (size_t)NB * TH * 32 * TEMPORAL_V * sizeof(word); }
+
+    static cudaError_t prepare_batch(int layout, int TH) {
+        const int smem = (int)tile_smem(TH);
+        switch (layout) {
+            case LAYOUT_LINEAR:
+                return cudaFuncSetAttribute(batch_kernel<LAYOUT_LINEAR>(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            case LAYOUT_TILED4:
+                return cudaFuncSetAttribute(batch_kernel<LAYOUT_TILED4>(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            case LAYOUT_TILED8:
+                return cudaFuncSetAttribute(batch_kernel<LAYOUT_TILED8>(), cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        }
+        return cudaErrorInvalidValue;
+    }
+
+    static cudaError_t temporal_batch(int layout, const batch_grid_desc* grids, const batch_item* items, int n_items,
+                                      int parity, int t0, int TH, int HY, int ctas, cudaStream_t s) {
+        const size_t smem = tile_smem(TH);
+        const dim3 block(TEMPORAL_WARPS * 32), grid(ctas);
+        switch (layout) {
+            case LAYOUT_LINEAR:
+                batch_kernel<LAYOUT_LINEAR>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY);
+                break;
+            case LAYOUT_TILED4:
+                batch_kernel<LAYOUT_TILED4>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY);
+                break;
+            case LAYOUT_TILED8:
+                batch_kernel<LAYOUT_TILED8>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY);
+                break;
+            default:
+                return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+
     static rule_ops ops() {
         return rule_ops{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS,
-                        &take_wait_timeouts};
+                        &take_wait_timeouts, &prepare_batch, &temporal_batch};
     }
 };
 

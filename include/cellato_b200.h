@@ -157,6 +157,36 @@ int cellato_set_simple_variant(int variant);
  * counterpart in the reference, whose kernels never wait. */
 int cellato_device_wait_timeouts(unsigned* count);
 
+/* ---- batches: many independent grids per launch -------------------------
+ * No counterpart in the reference (one grid per traverser run).  Results are
+ * identical to cellato_run_temporal on each grid alone with the same k. */
+
+typedef struct cellato_batch_st* cellato_batch_t;
+
+typedef struct {
+    int rule;                /* cellato_rule */
+    int x_cells, y_cells;    /* accepted by cellato_check_dims for the batch's layout */
+    int steps;               /* this grid's steps per launch of the batch (>= 0) */
+    void* planes_a[8];       /* input planes (first rule_planes entries used) */
+    void* planes_b[8];       /* second buffer of the ping-pong */
+} cellato_batch_grid;
+
+/* Plans a batch: grids of one rule advance k_per_rule[rule] steps per round
+ * (NULL or 0 entries: 8), one batched launch per round covers every tile of
+ * every grid of that rule still running, the rules' chains of rounds become
+ * parallel branches of one CUDA graph (built and instantiated here).  Allocates
+ * the work lists on the device.  Grids steps count from 0 (step parity as a run
+ * with t0 = 0). */
+int cellato_batch_create(int layout, int word_bits, const cellato_batch_grid* grids, int n_grids,
+                         const int* k_per_rule, cellato_batch_t* out);
+/* One graph launch: every grid advances its `steps` (ping-pong a -> b -> ...). */
+int cellato_batch_launch(cellato_batch_t batch, cellato_stream_t stream);
+/* 1 when grid's result is in planes_b after a launch (odd number of rounds). */
+int cellato_batch_result_in_b(cellato_batch_t batch, int grid, int* in_b);
+/* Kernel launches in the graph and work items (tiles x rounds) of the batch. */
+int cellato_batch_info(cellato_batch_t batch, int* kernel_launches, long long* work_items);
+int cellato_batch_destroy(cellato_batch_t batch);
+
 /* Largest tile_rows the temporal kernel accepts for (rule, layout, word_bits)
  * on the current device, or a negative status. */
 int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits);
