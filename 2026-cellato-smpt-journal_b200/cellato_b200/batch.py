@@ -55,3 +55,24 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def run_noalloc(layout: int, word_bits: int, grids, k_per_rule=None, stream: int = 0):
+    """cellato_batch_run_noalloc: the batched run with its work list in the
+    library's fixed device array (no device allocation).  grids as for Batch;
+    returns the per-grid result_in_b flags."""
+    L = lib.load()
+    arr = (lib.BatchGrid * max(1, len(grids)))()
+    for i, (rule, X, Y, steps, pa, pb) in enumerate(grids):
+        arr[i].rule = lib.rule_id(rule)
+        arr[i].x_cells, arr[i].y_cells, arr[i].steps = X, Y, steps
+        for p, ptr in enumerate(pa):
+            arr[i].planes_a[p] = ptr
+        for p, ptr in enumerate(pb):
+            arr[i].planes_b[p] = ptr
+    ks = None
+    if k_per_rule is not None:
+        ks = (ctypes.c_int * 10)(*[int(k_per_rule.get(r, 0)) for r in range(10)])
+    flags = (ctypes.c_int * max(1, len(grids)))()
+    lib.check(L.cellato_batch_run_noalloc(layout, word_bits, arr, len(grids), ks, stream, flags))
+    return [flags[i] for i in range(len(grids))]

@@ -29,7 +29,7 @@ EXPORTED = [
     "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
     "cellato_device_wait_timeouts", "cellato_set_simple_variant",
     "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
-    "cellato_batch_destroy",
+    "cellato_batch_destroy", "cellato_batch_run_noalloc",
 ]
 
 
@@ -75,6 +75,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cellato_batch_result_in_b.argtypes = [_vp, i, ctypes.POINTER(i)]
     lib.cellato_batch_info.argtypes = [_vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]
     lib.cellato_batch_destroy.argtypes = [_vp]
+    lib.cellato_batch_run_noalloc.argtypes = [i, i, ctypes.POINTER(BatchGrid), i, ctypes.POINTER(ctypes.c_int), _vp,
+                                              ctypes.POINTER(ctypes.c_int)]
     lib.cellato_pack_cells.argtypes = [i, i, i, _vp, i, i, _PP, _vp]
     lib.cellato_unpack_cells.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
     _lib = lib

@@ -187,6 +187,33 @@ int cellato_batch_result_in_b(cellato_batch_t batch, int grid, int* in_b);
 int cellato_batch_info(cellato_batch_t batch, int* kernel_launches, long long* work_items);
 int cellato_batch_destroy(cellato_batch_t batch);
 
+/* ---- batched run without device allocation ------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory -- a host framework or plugin host that owns all device memory through
+ * its own pool, a latency-critical loop that cannot afford cudaMalloc's implicit
+ * synchronisation, code held to a fixed device-memory budget.  Runs the same
+ * batched temporal kernels as cellato_batch_create + cellato_batch_launch (same
+ * results), with the work list kept in a fixed array in the library's device
+ * memory (CELLATO_NOALLOC_MAX_GRIDS descriptors and CELLATO_NOALLOC_MAX_ITEMS
+ * work items, about 1.2 MB, held by every GPU that loads the library until the
+ * process exits) instead of a cudaMalloc'd one; no CUDA graph, stream or event
+ * is created, kernels are launched in order on `stream`.  Calls no cudaMalloc or
+ * cudaFree.
+ *   - grids: as for cellato_batch_create; result_in_b: n_grids ints (host),
+ *     set to 1 where a grid's result is in planes_b.
+ *   - More than CELLATO_NOALLOC_MAX_GRIDS grids or CELLATO_NOALLOC_MAX_ITEMS
+ *     work items (tiles x rounds over the batch): CELLATO_EINVAL, nothing runs.
+ *   - The first call on a device looks up the array's device address (with
+ *     cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the array and it keeps the last call's work list; each
+ *     call writes the whole list it uses before its kernels (stream-ordered).
+ *     Calls whose work can overlap on the GPU (other streams, other threads)
+ *     race on the array: serialise them. */
+#define CELLATO_NOALLOC_MAX_GRIDS 1024
+#define CELLATO_NOALLOC_MAX_ITEMS 65536
+int cellato_batch_run_noalloc(int layout, int word_bits, const cellato_batch_grid* grids, int n_grids,
+                              const int* k_per_rule, cellato_stream_t stream, int* result_in_b);
+
 /* Largest tile_rows the temporal kernel accepts for (rule, layout, word_bits)
  * on the current device, or a negative status. */
 int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits);
