@@ -40,6 +40,7 @@ CA_STEPS = 1000
 LAYOUT = 1        # tiled_bit_planes
 WORD_BITS = 64
 SEED = 42
+BATCH_CANDIDATES = (("temporal", 2), ("temporal", 4), ("temporal", 8), ("temporal", 12), ("temporal", 16))
 CPU_SAMPLE_SIZE = 2048
 
 # DRAM bytes (read + write) per launch measured by one ncu capture of the same
@@ -59,6 +60,13 @@ def parse():
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--ca-steps", type=int, default=CA_STEPS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="config2", choices=["config2", "batched"],
+                    help="config2: WireWorld + Greenberg-Hastings 16384^2 x 1000 steps (default); "
+                         "batched: many mixed grids in one CUDA-graph launch vs per-grid launches")
+    ap.add_argument("--batch-grids", type=int, default=4096)
+    ap.add_argument("--batch-min-side", type=int, default=64)
+    ap.add_argument("--batch-max-side", type=int, default=4096)
+    ap.add_argument("--batch-max-steps", type=int, default=1000)
     return ap.parse_args()
 
 
@@ -385,6 +393,133 @@ def our_arm(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- batched workload
+def batched_arm(args, rank: int, world: int):
+    """Many independent grids (mixed automata, log-uniform sides, aspect 1-4,
+    uniform step counts) advanced by one CUDA-graph launch of the batch,
+    against the same grids run one after another with per-grid launches."""
+    import numpy as np
+    import torch
+    from cellato_b200 import inputs, lib
+    from cellato_b200.batch import Batch
+    from cellato_b200.device import DevicePlanes
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(SEED + rank)
+    layout, W = LAYOUT, WORD_BITS
+    R = W // 8
+    specs = []
+    lo, hi = np.log(args.batch_min_side), np.log(args.batch_max_side)
+    for _ in range(args.batch_grids):
+        rule = int(rng.integers(0, 10))
+        side = float(np.exp(rng.uniform(lo, hi)))
+        aspect = float(rng.uniform(1.0, 4.0))
+        X, Y = side * np.sqrt(aspect), side / np.sqrt(aspect)
+        if rng.integers(0, 2):
+            X, Y = Y, X
+        X = max(64, int(round(X / 64)) * 64)          # quantised to the layout: X multiple of 64,
+        Y = max(2 * R, int(round(Y / (2 * R))) * 2 * R)  # Y multiple of 2 tile rows (even for critters)
+        steps = int(rng.integers(10, args.batch_max_steps + 1))
+        specs.append((rule, X, Y, steps))
+    # device-generated seeded inputs at each automaton's reference density
+    bufs = []
+    g = torch.Generator(device=dev)
+    for i, (rule, X, Y, steps) in enumerate(specs):
+        name = inputs.RULES[rule]
+        probs = inputs.REFERENCE_DENSITY[name]
+        vals = torch.tensor(list(probs.keys()), dtype=torch.uint8, device=dev)
+        cum = torch.tensor(np.cumsum(list(probs.values())), dtype=torch.float64, device=dev)
+        g.manual_seed(SEED * 100003 + i)
+        u = torch.rand((Y, X), generator=g, device=dev, dtype=torch.float64)
+        k = torch.clamp(torch.bucketize(u, cum), max=len(vals) - 1)
+        cells = vals[k].contiguous()
+        nb = inputs.PLANES[rule]
+        a, b = DevicePlanes(nb, X, Y, dev), DevicePlanes(nb, X, Y, dev)
+        a.pack_from(cells, layout, W)
+        init = DevicePlanes(nb, X, Y, dev)
+        init.buf.copy_(a.buf)
+        bufs.append((a, b, init))
+    torch.cuda.synchronize()
+    # temporal depth per automaton from the autotuner, measured on scratch copies of the
+    # median-sized grid of that automaton in the batch
+    from cellato_b200 import autotune
+    ks = {}
+    for r in sorted({s[0] for s in specs}):
+        mine = sorted((X * Y, i) for i, (rr, X, Y, _) in enumerate(specs) if rr == r)
+        i = mine[len(mine) // 2][1]
+        _, X, Y, _ = specs[i]
+        sa, sb = DevicePlanes(inputs.PLANES[r], X, Y, dev), DevicePlanes(inputs.PLANES[r], X, Y, dev)
+        sa.buf.copy_(bufs[i][0].buf)
+        choice = autotune.tune(r, layout, W, sa.ptrs, sb.ptrs, X, Y, candidates=BATCH_CANDIDATES, use_cache=False)
+        ks[r] = choice["k"]
+        del sa, sb
+    cells_total = sum(X * Y * s for _, X, Y, s in specs)
+
+    batch = Batch(layout, W, [(r, X, Y, s, a.ptrs, b.ptrs) for (r, X, Y, s), (a, b, _) in zip(specs, bufs)], ks)
+    info = batch.info()
+    sp = stream.cuda_stream
+    for _ in range(args.warmup):
+        batch.launch(sp)
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch.launch(sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_batched = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+
+    # results of one batched launch from the initial state, for the comparison
+    for a, b, init in bufs:
+        a.buf.copy_(init.buf)
+    batch.launch(sp)
+    torch.cuda.synchronize()
+    batched_out = [((b if batch.result_in_b(i) else a).buf.clone()) for i, (a, b, _) in enumerate(bufs)]
+
+    # plain per-grid launches of the same work
+    for a, b, init in bufs:
+        a.buf.copy_(init.buf)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    in_b = []
+    for (rule, X, Y, s), (a, b, _) in zip(specs, bufs):
+        in_b.append(lib.run_temporal(rule, layout, W, a.ptrs, b.ptrs, X, Y, 0, s, ks[rule], 0, sp))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_per_grid = e0.elapsed_time(e1)
+    mismatches = sum(0 if torch.equal(((b if f else a).buf), out) else 1
+                     for (a, b, _), f, out in zip(bufs, in_b, batched_out))
+    per_grid_launches = sum(-(-s // ks[r]) for r, _, _, s in specs)
+
+    if rank != 0:
+        return
+    value = cells_total * world / (ms_batched * 1e-3) / 1e9
+    per_grid = cells_total / (ms_per_grid * 1e-3) / 1e9
+    line = {
+        "metric": "GCUPS", "value": round(value, 1), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_batched, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded, device-generated at reference densities)",
+        "config": {"workload": f"batched: {args.batch_grids} grids, sides log-uniform {args.batch_min_side}-"
+                               f"{args.batch_max_side}, aspect 1-4, 10 automata uniform, steps uniform "
+                               f"10-{args.batch_max_steps}; tiled_bit_planes W64, k autotuned per automaton; one CUDA-graph launch",
+                   "k_per_automaton": {inputs.RULES[r]: k for r, k in ks.items()},
+                   "quantisation": "X to a multiple of 64, Y to a multiple of 16",
+                   "cells_updates_per_step": cells_total, "graph_kernel_launches": info["kernel_launches"],
+                   "work_items": info["work_items"]},
+        "per_grid_launches_gcups": round(per_grid, 1),
+        "batched_over_per_grid": round(value / world / per_grid, 2),
+        "per_grid_kernel_launches": per_grid_launches,
+        "bit_exact_vs_per_grid": mismatches == 0, "mismatching_grids": mismatches,
+        "e2e": None, "e2e_note": "device-resident workload; see the config2 line for end-to-end",
+        "gpu_launches": info["kernel_launches"] * args.steps,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -416,6 +551,8 @@ def main():
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)
+        elif args.workload == "batched":
+            batched_arm(args, rank, world)
         else:
             our_arm(args, rank, world)
     finally:
