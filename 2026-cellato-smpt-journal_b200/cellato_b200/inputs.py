@@ -98,3 +98,15 @@ def workload_grid(name: str, X: int, Y: int, seed: int) -> np.ndarray:
 
 def reference_density_grid(name: str, X: int, Y: int, seed: int) -> np.ndarray:
     return categorical(X, Y, REFERENCE_DENSITY[name], seed)
+
+
+def thresholds(probs: dict) -> list:
+    """Thresholds of the device generator (cellato_fill_random) for index
+    probabilities {index: p}: t_i = floor(P(index <= i) * 2^32) for i below the
+    last index with p > 0, so that index = #{i : t_i <= u} for a uniform u32."""
+    last = max(i for i, p in probs.items() if p > 0)
+    out, cum = [], 0.0
+    for i in range(last):
+        cum += probs.get(i, 0.0)
+        out.append(min(int(cum * 2.0 ** 32), 2 ** 32 - 1))
+    return out

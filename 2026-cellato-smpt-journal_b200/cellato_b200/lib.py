@@ -30,6 +30,10 @@ EXPORTED = [
     "cellato_device_wait_timeouts", "cellato_set_simple_variant",
     "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
     "cellato_batch_destroy", "cellato_batch_run_noalloc",
+    "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random",
+    "cellato_server_create", "cellato_server_submit_random", "cellato_server_submit_planes",
+    "cellato_server_iterate", "cellato_server_poll", "cellato_server_planes", "cellato_server_release",
+    "cellato_server_stats_get", "cellato_server_destroy",
 ]
 
 
@@ -42,6 +46,25 @@ class CellatoError(RuntimeError):
 class BatchGrid(ctypes.Structure):
     _fields_ = [("rule", ctypes.c_int), ("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int),
                 ("steps", ctypes.c_int), ("planes_a", ctypes.c_void_p * 8), ("planes_b", ctypes.c_void_p * 8)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("layout", ctypes.c_int), ("word_bits", ctypes.c_int), ("hbm_cap_bytes", ctypes.c_ulonglong),
+                ("tile_budget", ctypes.c_int), ("chunk_rounds", ctypes.c_int), ("max_inflight", ctypes.c_int),
+                ("k_per_rule", ctypes.c_int * 10)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_longlong), ("rule", ctypes.c_int), ("x_cells", ctypes.c_int),
+                ("y_cells", ctypes.c_int), ("steps", ctypes.c_int), ("result_in_b", ctypes.c_int),
+                ("checksum", ctypes.c_ulonglong * 16), ("submit_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("waiting", ctypes.c_longlong), ("running", ctypes.c_longlong), ("active", ctypes.c_longlong),
+                ("completed_unpolled", ctypes.c_longlong), ("resident_bytes", ctypes.c_ulonglong),
+                ("hbm_cap_bytes", ctypes.c_ulonglong), ("iterations", ctypes.c_longlong),
+                ("kernel_launches", ctypes.c_longlong), ("cell_steps", ctypes.c_double)]
 
 
 _lib = None
@@ -79,6 +102,21 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                               ctypes.POINTER(ctypes.c_int)]
     lib.cellato_pack_cells.argtypes = [i, i, i, _vp, i, i, _PP, _vp]
     lib.cellato_unpack_cells.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    ll = ctypes.c_longlong
+    lib.cellato_checksum.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
+    lib.cellato_rule_state_value.argtypes = [i, i, ctypes.POINTER(ll)]
+    lib.cellato_fill_random.argtypes = [i, i, i, _PP, i, i, ctypes.c_ulonglong, u32p, i, _vp]
+    lib.cellato_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]
+    lib.cellato_server_submit_random.argtypes = [_vp, i, i, i, i, ctypes.c_ulonglong, u32p, i, i,
+                                                 ctypes.POINTER(ll)]
+    lib.cellato_server_submit_planes.argtypes = [_vp, i, i, i, i, _PP, i, ctypes.POINTER(ll)]
+    lib.cellato_server_iterate.argtypes = [_vp, ctypes.POINTER(i)]
+    lib.cellato_server_poll.argtypes = [_vp, ctypes.POINTER(ServerResult), i, ctypes.POINTER(i)]
+    lib.cellato_server_planes.argtypes = [_vp, ll, _PP]
+    lib.cellato_server_release.argtypes = [_vp, ll]
+    lib.cellato_server_stats_get.argtypes = [_vp, ctypes.POINTER(ServerStats)]
+    lib.cellato_server_destroy.argtypes = [_vp]
     _lib = lib
     return lib
 
@@ -155,3 +193,36 @@ def run_temporal(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, 
     check(load().cellato_run_temporal(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),
                                       X, Y, t0, steps, k, tile_rows, stream, ctypes.byref(out)))
     return out.value
+
+
+def checksum(rule, layout: int, word_bits: int, planes, X: int, Y: int, sums_ptr: int, stream: int = 0) -> None:
+    """4 x 4 tile sums of the state values into 16 uint64 of device memory at sums_ptr."""
+    check(load().cellato_checksum(rule_id(rule), layout, word_bits, ptr_array(planes), X, Y, sums_ptr, stream))
+
+
+def state_value(rule, index: int) -> int:
+    v = ctypes.c_longlong()
+    check(load().cellato_rule_state_value(rule_id(rule), index, ctypes.byref(v)))
+    return v.value
+
+
+def fill_random(layout: int, word_bits: int, nb: int, planes, X: int, Y: int, seed: int, thresholds,
+                stream: int = 0) -> None:
+    """Seeded i.i.d. initial state straight into nb device planes (see cellato_fill_random)."""
+    th = (ctypes.c_uint32 * max(1, len(thresholds)))(*thresholds)
+    check(load().cellato_fill_random(layout, word_bits, nb, ptr_array(planes), X, Y, seed, th, len(thresholds),
+                                     stream))
+
+
+def checksum_string(sums) -> str:
+    """The reference's printed form of the 16 tile sums."""
+    return "-".join(str(int(v)) for v in sums)
+
+
+def download_planes(nb: int, dev_ptrs, plane_bytes: int, stream: int = 0):
+    """Copy nb device planes into a new (nb, plane_bytes) uint8 host array (synchronous)."""
+    import numpy as np
+    out = np.empty((nb, plane_bytes), dtype=np.uint8)
+    host = ptr_array([out[p].ctypes.data for p in range(nb)])
+    check(load().cellato_planes_download(nb, host, ptr_array(dev_ptrs), plane_bytes, stream))
+    return out

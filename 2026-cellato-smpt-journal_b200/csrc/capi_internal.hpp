@@ -1,8 +1,11 @@
-// Helpers shared by the C ABI translation units (capi.cu, batch.cu).
+// Helpers shared by the C ABI translation units (capi.cu, batch.cu, noalloc.cu,
+// grid_ops.cu, serve.cu).
 #ifndef CELLATO_B200_CAPI_INTERNAL_HPP
 #define CELLATO_B200_CAPI_INTERNAL_HPP
 
 #include <cuda_runtime.h>
+
+#include <cstdint>
 
 #include "rule_kernels.cuh"
 
@@ -15,6 +18,11 @@ int band_height(int layout, int word_bits);
 int check_dims(int layout, int word_bits, int X, int Y);
 int make_sets(const rule_ops* ops, void* const* a, void* const* b, plane_set& pa, plane_set& pb);
 int default_tile_rows(const rule_ops* ops, int R);
+// grid_ops.cu: stream-ordered checksum (16 device uint64) and random fill
+int enqueue_checksum(const rule_ops* ops, int layout, int word_bits, const plane_set& ps, int X, int Y,
+                     unsigned long long* out, cudaStream_t s);
+int enqueue_fill_random(int layout, int word_bits, int nb, const plane_set& ps, int X, int Y, unsigned long long seed,
+                        const uint32_t* thresholds, int n_thresholds, cudaStream_t s);
 }  // namespace cellato::b200::capi
 
 #endif

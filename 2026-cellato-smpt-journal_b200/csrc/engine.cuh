@@ -783,16 +783,25 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
 // Many independent grids of one rule in one launch: persistent CTAs stride over
 // a device work list of (grid, tile, steps) items and run the temporal tile of
 // each item.  Every grid has its own planes (p[0] = a, p[1] = b), sizes and
-// step budget; all items of a launch start at the same global step t0 and use
-// the launch's halo HY, which covers their step count (steps <= k).
+// step budget; all items use the launch's halo HY, which covers their step
+// count (steps <= k).  By default all items read p[parity] and start at the
+// launch's global step t0.  Two flag bits above the step count let items of one
+// launch sit at different points of their runs (a server advancing requests
+// admitted at different times): BATCH_FLIP_BUFFER reads p[parity ^ 1] instead,
+// BATCH_FLIP_TIME starts at t0 + 1.  Only the parity of a step number matters
+// to the rules (alternation and Margolus phase), so one bit covers any start.
 struct batch_grid_desc {
     plane_set p[2];
     int Xw, Y;
 };
 
 struct batch_item {
-    int grid, tx, ty, steps;
+    int grid, tx, ty, steps;  // steps: count in the low 8 bits, then the flags
 };
+
+constexpr int BATCH_STEPS_MASK = 0xff;
+constexpr int BATCH_FLIP_BUFFER = 1 << 8;
+constexpr int BATCH_FLIP_TIME = 1 << 9;
 
 template <class Net, int NB, int LAYOUT, int V, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) temporal_batch_kernel(const batch_grid_desc* __restrict__ grids,
@@ -801,8 +810,10 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_batch_kernel(const batch_
     for (int i = blockIdx.x; i < n_items; i += gridDim.x) {
         const batch_item it = items[i];
         const batch_grid_desc& g = grids[it.grid];
-        temporal_tile<Net, NB, LAYOUT, V, WARPS>(g.p[parity], g.p[parity ^ 1], g.Xw, g.Y, t0, it.steps, TH, HY, it.tx,
-                                                  it.ty);
+        const int src = parity ^ ((it.steps & BATCH_FLIP_BUFFER) ? 1 : 0);
+        const int start = t0 + ((it.steps & BATCH_FLIP_TIME) ? 1 : 0);
+        temporal_tile<Net, NB, LAYOUT, V, WARPS>(g.p[src], g.p[src ^ 1], g.Xw, g.Y, start, it.steps & BATCH_STEPS_MASK,
+                                                  TH, HY, it.tx, it.ty);
         __syncthreads();  // the next item reloads the tile
     }
 }

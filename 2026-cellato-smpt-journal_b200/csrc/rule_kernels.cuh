@@ -41,6 +41,8 @@ struct rule_ops {
     cudaError_t (*prepare_batch)(int layout, int TH);
     cudaError_t (*temporal_batch)(int layout, const batch_grid_desc* grids, const batch_item* items, int n_items,
                                   int parity, int t0, int TH, int HY, int ctas, cudaStream_t s);
+    // state value of each dictionary index (index_to_state), 0 past `states`
+    long long state_values[32];
 };
 
 // Words per lane of the single-step kernel: as wide as registers allow.  A row
@@ -203,8 +205,12 @@ struct rule_kernels {
     }
 
     static rule_ops ops() {
-        return rule_ops{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS,
-                        &take_wait_timeouts, &prepare_batch, &temporal_batch};
+        rule_ops o{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS,
+                   &take_wait_timeouts, &prepare_batch, &temporal_batch, {}};
+        static_assert(dict::number_of_values <= 32, "state table holds 32 values");
+        for (int i = 0; i < dict::number_of_values; ++i)
+            o.state_values[i] = static_cast<long long>(dict::index_to_state(i));
+        return o;
     }
 };
 

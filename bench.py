@@ -60,13 +60,22 @@ def parse():
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--ca-steps", type=int, default=CA_STEPS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config2", choices=["config2", "batched"],
+    ap.add_argument("--workload", default="config2", choices=["config2", "batched", "served"],
                     help="config2: WireWorld + Greenberg-Hastings 16384^2 x 1000 steps (default); "
-                         "batched: many mixed grids in one CUDA-graph launch vs per-grid launches")
+                         "batched: many mixed grids in one CUDA-graph launch vs per-grid launches; "
+                         "served: a Poisson request stream through the continuous-batching server")
     ap.add_argument("--batch-grids", type=int, default=4096)
     ap.add_argument("--batch-min-side", type=int, default=64)
     ap.add_argument("--batch-max-side", type=int, default=4096)
     ap.add_argument("--batch-max-steps", type=int, default=1000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="length of the arrival window, s")
+    ap.add_argument("--serve-min-side", type=int, default=128)
+    ap.add_argument("--serve-max-side", type=int, default=8192)
+    ap.add_argument("--serve-min-steps", type=int, default=100)
+    ap.add_argument("--serve-max-steps", type=int, default=10000)
+    ap.add_argument("--serve-check-fraction", type=float, default=0.01)
+    ap.add_argument("--no-per-grid", action="store_true", help="served: skip the per-grid baseline run")
     return ap.parse_args()
 
 
@@ -520,6 +529,159 @@ def batched_arm(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def tune_temporal_k(dev, layout: int, W: int, sides) -> dict:
+    """Temporal depth per automaton from the autotuner, measured on a scratch
+    grid of each automaton at the given (X, Y)."""
+    from cellato_b200 import autotune, inputs, lib
+    from cellato_b200.device import DevicePlanes
+    ks = {}
+    for r, (X, Y) in sides.items():
+        nb = inputs.PLANES[r]
+        sa, sb = DevicePlanes(nb, X, Y, dev), DevicePlanes(nb, X, Y, dev)
+        lib.fill_random(layout, W, nb, sa.ptrs, X, Y, SEED + r,
+                        inputs.thresholds(inputs.REFERENCE_DENSITY[inputs.RULES[r]]))
+        ks[r] = autotune.tune(r, layout, W, sa.ptrs, sb.ptrs, X, Y, candidates=BATCH_CANDIDATES,
+                              use_cache=False)["k"]
+        del sa, sb
+    return ks
+
+
+def served_arm(args, rank: int, world: int):
+    """A Poisson stream of simulation requests through the continuous-batching
+    server (cellato_server_*), then the same stream served one request at a time
+    with plain per-grid launches.  Latency is measured from each request's
+    scheduled arrival to the moment the host has its result (the 16 tile sums)."""
+    import numpy as np
+    import torch
+    from cellato_b200 import inputs, lib
+    from cellato_b200.device import DevicePlanes
+    from cellato_b200.serve import Server
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    layout, W = LAYOUT, WORD_BITS
+    rng = np.random.default_rng(SEED + 7 + rank)
+    # arrivals over the window; sides and steps log-uniform; automata uniform
+    t, arrivals = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / args.serve_rate))
+        if t > args.serve_seconds:
+            break
+        arrivals.append(t)
+    n = len(arrivals)
+    reqs = []
+    ls0, ls1 = np.log(args.serve_min_side), np.log(args.serve_max_side)
+    lt0, lt1 = np.log(args.serve_min_steps), np.log(args.serve_max_steps)
+    for i in range(n):
+        r = int(rng.integers(0, 10))
+        side = float(np.exp(rng.uniform(ls0, ls1)))
+        X = max(64, int(round(side / 64)) * 64)
+        Y = max(16, int(round(side / 16)) * 16)
+        steps = int(round(np.exp(rng.uniform(lt0, lt1))))
+        reqs.append((r, X, Y, steps, SEED * 1000003 + i))
+    ths = {r: inputs.thresholds(inputs.REFERENCE_DENSITY[inputs.RULES[r]]) for r in range(10)}
+    cell_updates = sum(X * Y * s for _, X, Y, s, _ in reqs)
+    n_sample = min(n, max(3, int(round(n * args.serve_check_fraction))))
+    sample = sorted(int(i) for i in rng.choice(n, size=n_sample, replace=False))
+    ks = tune_temporal_k(dev, layout, W, {r: (1024, 1024) for r in range(10)})
+    torch.cuda.synchronize()
+
+    # ---- served
+    with ClockSampler(dev.index) as clocks:
+        srv = Server(layout, W, k_per_rule=ks)
+        lat, sums, ids = {}, {}, {}
+        keep = set(sample)
+        i = 0
+        t0 = time.perf_counter()
+        while len(lat) < n:
+            now = time.perf_counter() - t0
+            while i < n and arrivals[i] <= now:
+                r, X, Y, steps, seed = reqs[i]
+                ids[srv.submit_random(r, X, Y, steps, seed, thresholds=ths[r], keep=i in keep)] = i
+                i += 1
+            active = srv.iterate()
+            for res in srv.poll():
+                j = ids[res["id"]]
+                lat[j] = time.perf_counter() - t0 - arrivals[j]
+                sums[j] = res["checksum"]
+            if active == 0 and srv.pending() == 0 and i < n:
+                time.sleep(max(0.0, arrivals[i] - (time.perf_counter() - t0)))
+        makespan = time.perf_counter() - t0
+    stats = srv.stats()
+    rid_of = {j: rid for rid, j in ids.items()}
+
+    # ---- the sample: served planes against the same request run alone
+    sample_ok = 0
+    for j in sample:
+        r, X, Y, steps, seed = reqs[j]
+        nb = inputs.PLANES[r]
+        a, b = DevicePlanes(nb, X, Y, dev), DevicePlanes(nb, X, Y, dev)
+        lib.fill_random(layout, W, nb, a.ptrs, X, Y, seed, ths[r])
+        in_b = lib.run_temporal(r, layout, W, a.ptrs, b.ptrs, X, Y, 0, steps, ks[r])
+        alone = (b if in_b else a).download()
+        served = lib.download_planes(nb, srv.planes(rid_of[j], nb), X * Y // 8)
+        sample_ok += int(np.array_equal(alone, served))
+        srv.release(rid_of[j])
+        del a, b
+    srv.close()
+
+    # ---- the same stream, one request at a time with per-grid launches
+    base = None
+    if not args.no_per_grid:
+        base_lat, mism = [], 0
+        out = torch.zeros(16, dtype=torch.int64, device=dev)
+        t0 = time.perf_counter()
+        for j, (r, X, Y, steps, seed) in enumerate(reqs):
+            wait = arrivals[j] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            nb = inputs.PLANES[r]
+            a, b = DevicePlanes(nb, X, Y, dev), DevicePlanes(nb, X, Y, dev)
+            lib.fill_random(layout, W, nb, a.ptrs, X, Y, seed, ths[r])
+            in_b = lib.run_temporal(r, layout, W, a.ptrs, b.ptrs, X, Y, 0, steps, ks[r])
+            lib.checksum(r, layout, W, (b if in_b else a).ptrs, X, Y, out.data_ptr())
+            got = [int(v) & 0xFFFFFFFFFFFFFFFF for v in out.cpu().tolist()]
+            base_lat.append(time.perf_counter() - t0 - arrivals[j])
+            mism += int(got != sums[j])
+        base_span = time.perf_counter() - t0
+        base = {"gcups": round(cell_updates / base_span / 1e9, 1), "makespan_s": round(base_span, 3),
+                "p50_ms": round(1e3 * float(np.percentile(base_lat, 50)), 1),
+                "p99_ms": round(1e3 * float(np.percentile(base_lat, 99)), 1),
+                "checksum_mismatches_vs_served": mism}
+
+    if rank != 0:
+        return
+    lats = np.array([lat[j] for j in range(n)])
+    value = cell_updates * world / makespan / 1e9
+    line = {
+        "metric": "GCUPS", "value": round(value, 1), "unit": "GCUPS", "n_gpus": world, "steps": 1,
+        "warmup": 0, "ms_per_step": round(makespan * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded, device-generated at reference densities)",
+        "config": {"workload": f"served: Poisson {args.serve_rate:g} req/s for {args.serve_seconds:g} s "
+                               f"({n} requests), sides log-uniform {args.serve_min_side}-{args.serve_max_side}, "
+                               f"steps log-uniform {args.serve_min_steps}-{args.serve_max_steps}, 10 automata "
+                               f"uniform; tiled_bit_planes W64, k autotuned per automaton",
+                   "k_per_automaton": {inputs.RULES[r]: k for r, k in ks.items()},
+                   "quantisation": "X to a multiple of 64, Y to a multiple of 16",
+                   "cell_updates": cell_updates,
+                   "offered_gcups": round(cell_updates / args.serve_seconds / 1e9, 1),
+                   "timing": "host wall clock from the first scheduled arrival to the last result"},
+        "latency_ms": {"p50": round(1e3 * float(np.percentile(lats, 50)), 1),
+                       "p99": round(1e3 * float(np.percentile(lats, 99)), 1),
+                       "max": round(1e3 * float(lats.max()), 1)},
+        "per_grid": base,
+        "served_over_per_grid": round(value / world / base["gcups"], 2) if base else None,
+        "sample_bit_exact": f"{sample_ok}/{len(sample)}",
+        "server": {"iterations": stats["iterations"], "kernel_launches": stats["kernel_launches"]},
+        "e2e": {"value": round(value, 1), "unit": "GCUPS", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": 128 * n,
+                "note": "requests enter through the server's C ABI as seeds; results leave as 16 tile sums each"},
+        "gpu_launches": stats["kernel_launches"],
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -553,6 +715,8 @@ def main():
             reference_arm(args, rank, world)
         elif args.workload == "batched":
             batched_arm(args, rank, world)
+        elif args.workload == "served":
+            served_arm(args, rank, world)
         else:
             our_arm(args, rank, world)
     finally:

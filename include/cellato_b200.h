@@ -218,6 +218,111 @@ int cellato_batch_run_noalloc(int layout, int word_bits, const cellato_batch_gri
  * on the current device, or a negative status. */
 int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits);
 
+/* ---- whole-grid operations ----------------------------------------------- */
+
+/* The reference's grid checksum computed from the planes on the device
+ * (replaces standard_grid::get_checksum, include/memory/standard_grid.hpp:179-212,
+ * which needs the grid converted to one state value per cell on the host):
+ * sums[ty*4 + tx] = sum of the state values (not indices) of the cells of tile
+ * (tx, ty) of the 4 x 4 partition into ceil(X/4) x ceil(Y/4) tiles.  The
+ * reference prints the 16 sums joined by '-'.  sums: 16 uint64 in DEVICE
+ * memory, overwritten (stream-ordered, no allocation). */
+int cellato_checksum(int rule, int layout, int word_bits, const void* const* planes, int x_cells, int y_cells,
+                     unsigned long long* sums, cellato_stream_t stream);
+
+/* State value of dictionary index `index` of a rule (index_to_state,
+ * include/memory/state_dictionary.hpp:10-70). */
+int cellato_rule_state_value(int rule, int index, long long* value);
+
+/* Seeded random initial state written straight into nb device planes.  Cell
+ * (x, y) gets index #{i : thresholds[i] <= u}, u = upper 32 bits of the
+ * SplitMix64 output at seed + (y*X + x + 1) * 0x9E3779B97F4A7C15 (ascending
+ * thresholds, at most 31, fewer than 2^nb).  thresholds[i] =
+ * floor(P(index <= i) * 2^32) gives the indices their probabilities.  This is
+ * the library's own generator, not the reference's std::mt19937
+ * (include/memory/grid_utils.hpp:36-60); stream-ordered, no allocation. */
+int cellato_fill_random(int layout, int word_bits, int nb, void* const* planes, int x_cells, int y_cells,
+                        unsigned long long seed, const uint32_t* thresholds, int n_thresholds,
+                        cellato_stream_t stream);
+
+/* ---- simulation server: continuous batching of many requests ------------
+ * No counterpart in the reference (one grid per CLI run).  A request is one
+ * grid of one automaton advanced `steps` steps from step 0; the server keeps
+ * its planes resident on the device from admission to completion.
+ *   - Admission: strict FIFO in submission order while the planes of the
+ *     resident requests fit in hbm_cap_bytes (a stream-ordered memory pool owned
+ *     by the server holds them).
+ *   - Iteration (cellato_server_iterate): the resident requests, oldest first,
+ *     are activated while their temporal tiles fit in tile_budget; each active
+ *     request advances up to chunk_rounds rounds of k steps.  A round is one
+ *     batched temporal launch per automaton over the tiles of every active
+ *     request of it, the automata on parallel streams.  Requests join and leave
+ *     between iterations, at any step count.
+ *   - Completion: a finished request's checksum (as cellato_checksum) is
+ *     computed on the device and copied back; cellato_server_poll returns it.
+ *     Without `keep` its planes are freed at once; with `keep` they stay,
+ *     readable through cellato_server_planes, until cellato_server_release.
+ * Results are identical to cellato_run_temporal on each grid alone with the
+ * same k.  A server is used from one host thread at a time; all its device work
+ * is ordered on its own streams on the device current at creation. */
+
+typedef struct cellato_server_st* cellato_server_t;
+
+typedef struct {
+    int layout;                       /* cellato_layout */
+    int word_bits;                    /* 32 or 64 */
+    unsigned long long hbm_cap_bytes; /* resident plane bytes; 0: 80% of the device's memory */
+    int tile_budget;                  /* temporal tiles per round over all active requests; 0: 16 per SM */
+    int chunk_rounds;                 /* rounds per request per iteration; 0: 4 */
+    int max_inflight;                 /* iterations queued on the device at once; 0: 2 */
+    int k_per_rule[10];               /* temporal depth per rule, 1..32; 0: 16 */
+} cellato_server_config;
+
+typedef struct {
+    long long id;
+    int rule;
+    int x_cells, y_cells, steps;
+    int result_in_b;                  /* buffer holding the result (requests with keep) */
+    unsigned long long checksum[16];
+    double submit_s;                  /* server clock (seconds since creation) at submission */
+    double done_s;                    /* server clock when the host saw the result */
+} cellato_server_result;
+
+typedef struct {
+    long long waiting;                /* submitted, not admitted */
+    long long running;                /* admitted, steps left */
+    long long active;                 /* advanced by the last iteration */
+    long long completed_unpolled;
+    unsigned long long resident_bytes, hbm_cap_bytes;
+    long long iterations, kernel_launches;
+    double cell_steps;                /* cell updates enqueued since creation */
+} cellato_server_stats;
+
+int cellato_server_create(const cellato_server_config* config, cellato_server_t* out);
+/* Submit a request whose initial state is cellato_fill_random(seed, thresholds)
+ * (thresholds as there; NULL with n_thresholds = 0: all cells index 0). */
+int cellato_server_submit_random(cellato_server_t server, int rule, int x_cells, int y_cells, int steps,
+                                 unsigned long long seed, const uint32_t* thresholds, int n_thresholds, int keep,
+                                 long long* id);
+/* Submit a request whose initial state is given as rule_planes host planes in
+ * the server's layout (copied at submission). */
+int cellato_server_submit_planes(cellato_server_t server, int rule, int x_cells, int y_cells, int steps,
+                                 const void* const* host_planes, int keep, long long* id);
+/* One scheduling iteration: collect finished work, admit, plan and enqueue one
+ * chunk for the active requests.  Blocks only while max_inflight iterations are
+ * queued (or, with nothing to run, until the oldest queued one completes).
+ * *active = requests advanced by this iteration. */
+int cellato_server_iterate(cellato_server_t server, int* active);
+/* Moves up to `max` completed requests into out[]; *n = how many. */
+int cellato_server_poll(cellato_server_t server, cellato_server_result* out, int max, int* n);
+/* Device planes of a completed request submitted with keep (rule_planes entries). */
+int cellato_server_planes(cellato_server_t server, long long id, void** planes);
+/* Frees a completed request's planes (requests with keep). */
+int cellato_server_release(cellato_server_t server, long long id);
+int cellato_server_stats_get(cellato_server_t server, cellato_server_stats* stats);
+/* Waits for all queued work and frees everything the server holds. */
+int cellato_server_destroy(cellato_server_t server);
+
 #ifdef __cplusplus
 }
 #endif
