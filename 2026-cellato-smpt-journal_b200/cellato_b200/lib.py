@@ -33,7 +33,8 @@ EXPORTED = [
     "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random",
     "cellato_server_create", "cellato_server_submit_random", "cellato_server_submit_planes",
     "cellato_server_iterate", "cellato_server_poll", "cellato_server_planes", "cellato_server_release",
-    "cellato_server_stats_get", "cellato_server_destroy",
+    "cellato_server_stats_get", "cellato_server_destroy", "cellato_server_submit_resume",
+    "cellato_server_snapshot", "cellato_server_cancel",
 ]
 
 
@@ -117,6 +118,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cellato_server_release.argtypes = [_vp, ll]
     lib.cellato_server_stats_get.argtypes = [_vp, ctypes.POINTER(ServerStats)]
     lib.cellato_server_destroy.argtypes = [_vp]
+    lib.cellato_server_submit_resume.argtypes = [_vp, i, i, i, i, i, _PP, i, ctypes.POINTER(ll)]
+    lib.cellato_server_snapshot.argtypes = [_vp, ll, _PP, ctypes.POINTER(i), ctypes.POINTER(i)]
+    lib.cellato_server_cancel.argtypes = [_vp, ll]
     _lib = lib
     return lib
 

@@ -18,6 +18,8 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
+
 from . import inputs, lib
 
 
@@ -55,17 +57,35 @@ class Server:
         self._outstanding += 1
         return rid.value
 
-    def submit_planes(self, rule, X: int, Y: int, steps: int, host_planes, keep: bool = False) -> int:
+    def submit_planes(self, rule, X: int, Y: int, steps: int, host_planes, keep: bool = False,
+                      t0: int = 0) -> int:
         """A request whose initial state is given as host planes (numpy arrays,
-        one per plane, in the server's layout)."""
+        one per plane, in the server's layout), its first step numbered t0
+        (a snapshot's next_step when resuming)."""
         rule = lib.rule_id(rule)
-        arrs = [p for p in host_planes]
+        arrs = [np.ascontiguousarray(p) for p in host_planes]
         ptrs = (ctypes.c_void_p * max(1, len(arrs)))(*[a.ctypes.data for a in arrs])
         rid = ctypes.c_longlong()
-        lib.check(lib.load().cellato_server_submit_planes(self._h, rule, X, Y, steps, ptrs, int(keep),
+        lib.check(lib.load().cellato_server_submit_resume(self._h, rule, X, Y, steps, t0, ptrs, int(keep),
                                                           ctypes.byref(rid)))
         self._outstanding += 1
         return rid.value
+
+    def snapshot(self, rid: int, nb: int, X: int, Y: int):
+        """Checkpoint of a request: (planes as an (nb, X*Y/8) uint8 array,
+        steps done, next step number).  The request keeps running."""
+        out = np.empty((nb, X * Y // 8), dtype=np.uint8)
+        ptrs = (ctypes.c_void_p * 8)(*[out[p].ctypes.data for p in range(nb)])
+        done, nxt = ctypes.c_int(), ctypes.c_int()
+        lib.check(lib.load().cellato_server_snapshot(self._h, rid, ptrs, ctypes.byref(done), ctypes.byref(nxt)))
+        return out, done.value, nxt.value
+
+    def cancel(self, rid: int, completed: bool = False) -> None:
+        """Removes a request and frees its planes (pass completed=True for a
+        kept request whose result poll() already returned)."""
+        lib.check(lib.load().cellato_server_cancel(self._h, rid))
+        if not completed:
+            self._outstanding -= 1
 
     # -- progress
     def iterate(self) -> int:

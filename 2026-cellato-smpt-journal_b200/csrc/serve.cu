@@ -51,6 +51,7 @@ struct req_rec {
     int cur = 0;
     bool completed = false;
     double submit_s = 0;
+    int t0 = 0;  // number of the request's first step
 };
 
 struct slot {
@@ -159,6 +160,15 @@ int harvest_ready(cellato_server_st* s) {
     }
 }
 
+// Waits for every queued iteration and collects its results.
+int drain(cellato_server_st* s) {
+    while (!s->inflight.empty()) {
+        const int rc = harvest_one(s, true);
+        if (rc < 0) return -rc;
+    }
+    return CELLATO_OK;
+}
+
 int ensure_slot(cellato_server_st* s, slot& sl, size_t bytes) {
     if (sl.host_cap < bytes) {
         if (sl.host) cudaFreeHost(sl.host);
@@ -212,7 +222,8 @@ int materialise(cellato_server_st* s, long long id) {
     return CELLATO_OK;
 }
 
-int submit_common(cellato_server_t s, int rule, int x, int y, int steps, int keep, req_rec& r, long long* id) {
+int submit_common(cellato_server_t s, int rule, int x, int y, int steps, int t0, int keep, req_rec& r,
+                  long long* id) {
     if (!s || !id) return fail(CELLATO_EINVAL, "server and id must not be NULL");
     if (s->broken) return fail(CELLATO_ECUDA, "the server stopped after a CUDA error");
     const rule_ops* ops = ops_of(rule);
@@ -221,12 +232,13 @@ int submit_common(cellato_server_t s, int rule, int x, int y, int steps, int kee
     if (int rc = check_dims(s->layout, s->word_bits, x, y)) return rc;
     r.rule = rule, r.x = x, r.y = y, r.steps = steps, r.nb = ops->planes;
     r.keep = keep != 0;
+    r.t0 = t0;
     r.plane_bytes = (size_t)x * y / 8;
     r.stride = round_up(r.plane_bytes, ALIGN);
     const int effW = 32 * ops->temporal_words_per_lane - 2, effH = s->TH[rule] - 2 * s->HY[rule];
     const int tiles = ((x / 32 + effW - 1) / effW) * ((y + effH - 1) / effH);
     r.submit_s = s->now();
-    *id = s->sched.submit(rule, x, y, steps, (long long)(2 * (size_t)r.nb * r.stride), tiles, r.keep);
+    *id = s->sched.submit(rule, x, y, steps, (long long)(2 * (size_t)r.nb * r.stride), tiles, r.keep, t0 & 1);
     s->recs.emplace(*id, std::move(r));
     return CELLATO_OK;
 }
@@ -316,10 +328,10 @@ int cellato_server_submit_random(cellato_server_t s, int rule, int x, int y, int
     r.random = true;
     r.seed = seed;
     if (n_thresholds) r.thresholds.assign(thresholds, thresholds + n_thresholds);
-    return submit_common(s, rule, x, y, steps, keep, r, id);
+    return submit_common(s, rule, x, y, steps, 0, keep, r, id);
 }
 
-int cellato_server_submit_planes(cellato_server_t s, int rule, int x, int y, int steps,
+int cellato_server_submit_resume(cellato_server_t s, int rule, int x, int y, int steps, int t0,
                                  const void* const* host_planes, int keep, long long* id) {
     if (!s) return fail(CELLATO_EINVAL, "server is NULL");
     const rule_ops* ops = ops_of(rule);
@@ -334,7 +346,13 @@ int cellato_server_submit_planes(cellato_server_t s, int rule, int x, int y, int
         if (!host_planes[p]) return fail(CELLATO_EINVAL, "host plane %d is NULL", p);
         std::memcpy(r.host.data() + p * pb, host_planes[p], pb);
     }
-    return submit_common(s, rule, x, y, steps, keep, r, id);
+    if (t0 < 0) return fail(CELLATO_EINVAL, "negative start step");
+    return submit_common(s, rule, x, y, steps, t0, keep, r, id);
+}
+
+int cellato_server_submit_planes(cellato_server_t s, int rule, int x, int y, int steps,
+                                 const void* const* host_planes, int keep, long long* id) {
+    return cellato_server_submit_resume(s, rule, x, y, steps, 0, host_planes, keep, id);
 }
 
 int cellato_server_iterate(cellato_server_t s, int* active) {
@@ -491,6 +509,48 @@ int cellato_server_release(cellato_server_t s, long long id) {
     }
     s->sched.release(id);
     s->recs.erase(it);
+    return CELLATO_OK;
+}
+
+int cellato_server_snapshot(cellato_server_t s, long long id, void* const* host_planes, int* steps_done,
+                            int* next_step) {
+    if (!s || !host_planes) return fail(CELLATO_EINVAL, "server and host_planes must not be NULL");
+    if (s->broken) return fail(CELLATO_ECUDA, "the server stopped after a CUDA error");
+    if (int rc = drain(s)) return rc;
+    const sv::request* q = s->sched.find(id);
+    auto it = s->recs.find(id);
+    if (!q || it == s->recs.end() || q->ph == sv::phase::waiting || !it->second.base)
+        return fail(CELLATO_EINVAL, "request %lld has no state on the device (unknown, not admitted or freed)", id);
+    const req_rec& r = it->second;
+    for (int p = 0; p < r.nb; ++p) {
+        if (!host_planes[p]) return fail(CELLATO_EINVAL, "host plane %d is NULL", p);
+        const cudaError_t e = cudaMemcpyAsync(host_planes[p], r.p[q->cur].p[p], r.plane_bytes,
+                                              cudaMemcpyDeviceToHost, s->main_stream);
+        if (e != cudaSuccess) return server_cuda_fail(s, e, "cudaMemcpyAsync (snapshot)");
+    }
+    const cudaError_t e = cudaStreamSynchronize(s->main_stream);
+    if (e != cudaSuccess) return server_cuda_fail(s, e, "cudaStreamSynchronize (snapshot)");
+    if (steps_done) *steps_done = q->done;
+    if (next_step) *next_step = r.t0 + q->done;
+    return CELLATO_OK;
+}
+
+int cellato_server_cancel(cellato_server_t s, long long id) {
+    if (!s) return fail(CELLATO_EINVAL, "server is NULL");
+    if (s->broken) return fail(CELLATO_ECUDA, "the server stopped after a CUDA error");
+    if (int rc = drain(s)) return rc;
+    auto it = s->recs.find(id);
+    if (!s->sched.find(id) || it == s->recs.end()) return fail(CELLATO_EINVAL, "request %lld is not held", id);
+    if (it->second.base) {
+        const cudaError_t e = cudaFreeAsync(it->second.base, s->main_stream);
+        if (e != cudaSuccess) return server_cuda_fail(s, e, "cudaFreeAsync");
+    }
+    s->sched.cancel(id);
+    s->recs.erase(it);
+    // a result not yet polled goes too
+    s->completed.erase(std::remove_if(s->completed.begin(), s->completed.end(),
+                                      [id](const cellato_server_result& r) { return r.id == id; }),
+                       s->completed.end());
     return CELLATO_OK;
 }
 

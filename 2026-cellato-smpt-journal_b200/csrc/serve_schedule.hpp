@@ -3,8 +3,9 @@
 // continuous-batching iteration.  Host-only C++ with no CUDA dependency, so the
 // policy is unit-tested on its own.
 //
-// A request is a grid of one automaton to be advanced `steps` steps from step 0
-// (the reference runs one such grid per traverser call,
+// A request is a grid of one automaton to be advanced `steps` steps, numbered
+// from its start step t0 (0 for a new simulation, the step reached for one
+// resumed from a snapshot; the reference runs one such grid per traverser call,
 // include/traversers/cuda/temporal.cu:227-262; there is no server).  Its life:
 //   waiting   -- submitted, no device memory yet;
 //   resident  -- admitted: both plane buffers allocated and initialised.
@@ -37,6 +38,7 @@ enum class phase : int { waiting = 0, resident = 1, finished = 2 };
 struct request {
     long long id = 0;
     int rule = 0, x = 0, y = 0, steps = 0;
+    int t0 = 0;           // number of its first step (only the parity matters to the rules)
     long long bytes = 0;  // device footprint of both plane buffers
     int tiles = 0;        // temporal tiles per round
     bool keep = false;    // planes stay after finishing until released
@@ -82,10 +84,10 @@ public:
 
     const limits& lim() const { return lim_; }
 
-    long long submit(int rule, int x, int y, int steps, long long bytes, int tiles, bool keep) {
+    long long submit(int rule, int x, int y, int steps, long long bytes, int tiles, bool keep, int t0 = 0) {
         request r;
         r.id = next_id_++;
-        r.rule = rule, r.x = x, r.y = y, r.steps = steps;
+        r.rule = rule, r.x = x, r.y = y, r.steps = steps, r.t0 = t0;
         r.bytes = bytes, r.tiles = tiles, r.keep = keep;
         reqs_[r.id] = r;
         waiting_.push_back(r.id);
@@ -133,7 +135,7 @@ public:
             for (int s = 0, q = 0; s < chunk; s += k, ++q) {
                 const int n = std::min(k, chunk - s);
                 if ((int)rr.size() <= q) rr.emplace_back();
-                rr[q].push_back(round_entry{id, n, r.cur, r.done & 1});
+                rr[q].push_back(round_entry{id, n, r.cur, (r.t0 + r.done) & 1});
                 r.cur ^= 1;
                 r.done += n;
                 p.cell_steps += (long long)r.x * r.y * n;
@@ -158,6 +160,25 @@ public:
         if (it->second.keep) resident_bytes_ -= it->second.bytes;
         reqs_.erase(it);
         return true;
+    }
+
+    // Removes a request at any stage (preemption); its bytes leave the resident
+    // total.  Returns the phase it was in, or -1 when it is unknown.
+    int cancel(long long id) {
+        auto it = reqs_.find(id);
+        if (it == reqs_.end()) return -1;
+        const request& r = it->second;
+        const int ph = (int)r.ph;
+        if (r.ph == phase::waiting) {
+            waiting_.erase(std::find(waiting_.begin(), waiting_.end(), id));
+        } else if (r.ph == phase::resident) {
+            order_.erase(std::find(order_.begin(), order_.end(), id));
+            resident_bytes_ -= r.bytes;
+        } else if (r.keep) {
+            resident_bytes_ -= r.bytes;
+        }
+        reqs_.erase(it);
+        return ph;
     }
 
     const request* find(long long id) const {

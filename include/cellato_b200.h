@@ -308,6 +308,23 @@ int cellato_server_submit_random(cellato_server_t server, int rule, int x_cells,
  * the server's layout (copied at submission). */
 int cellato_server_submit_planes(cellato_server_t server, int rule, int x_cells, int y_cells, int steps,
                                  const void* const* host_planes, int keep, long long* id);
+/* Submit a request resumed from a snapshot: host planes of the state reached
+ * at step number t0 (cellato_server_snapshot's next_step), `steps` steps
+ * still to run.  The step parity continues from t0 as if never interrupted. */
+int cellato_server_submit_resume(cellato_server_t server, int rule, int x_cells, int y_cells, int steps, int t0,
+                                 const void* const* host_planes, int keep, long long* id);
+/* Snapshot (checkpoint) of a request on the device: waits for the server's
+ * queued iterations, copies the planes of the request's current state into
+ * rule_planes host buffers of x*y/8 bytes, and sets *steps_done (steps applied
+ * since submission) and *next_step (t0 + steps_done).  The request keeps
+ * running.  A request not yet admitted has no device state: CELLATO_EINVAL. */
+int cellato_server_snapshot(cellato_server_t server, long long id, void* const* host_planes, int* steps_done,
+                            int* next_step);
+/* Removes a request at any stage (waiting, running, or completed with keep)
+ * and frees its planes, after the server's queued work; a result of it that
+ * cellato_server_poll has not returned yet is dropped.  Snapshot, cancel and
+ * resume later is preemption without recomputation. */
+int cellato_server_cancel(cellato_server_t server, long long id);
 /* One scheduling iteration: collect finished work, admit, plan and enqueue one
  * chunk for the active requests.  Blocks only while max_inflight iterations are
  * queued (or, with nothing to run, until the oldest queued one completes).

@@ -9,8 +9,11 @@
 //     steps, read the buffers alternately starting with a, carry the parity of
 //     their first step number, and never exceed k steps;
 //   * every request finishes exactly once, with the final buffer = parity of
-//     its round count.
+//     its round count;
+//   * cancelling a request at any stage (preemption) removes it from the
+//     queues and its bytes from the resident total.
 // Prints "ok" and exits 0 on success; prints the failed check and exits 1.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -36,6 +39,7 @@ struct truth {
     long long bytes;
     int tiles;
     bool keep;
+    int t0 = 0;
     int done = 0, cur = 0, rounds = 0;
     bool finished = false, admitted = false;
 };
@@ -64,18 +68,39 @@ int scenario(unsigned seed, long long cap, long long budget, int chunk_rounds) {
             if (rng() % 50 == 0) q.bytes = cap + 5;  // larger than the cap
             q.tiles = 1 + (int)(rng() % 40);
             q.keep = rng() % 4 == 0;
-            const long long id = sch.submit(q.rule, 64, 64, q.steps, q.bytes, q.tiles, q.keep);
+            q.t0 = (int)(rng() % 4);
+            const long long id = sch.submit(q.rule, 64, 64, q.steps, q.bytes, q.tiles, q.keep, q.t0);
             t[id] = q;
             submitted.push_back(id);
         }
-        const long long before = sch.resident_bytes();
+        // now and then a live request is cancelled (preempted)
+        if (rng() % 8 == 0) {
+            std::vector<long long> live;
+            for (auto& [id, x] : t)
+                if (!x.finished) live.push_back(id);
+            if (!live.empty()) {
+                const long long id = live[rng() % live.size()];
+                truth& x = t[id];
+                const long long bytes = sch.resident_bytes();
+                const int ph = sch.cancel(id);
+                CHECK(ph == (x.admitted ? 1 : 0), "cancel of %lld reports phase %d", id, ph);
+                CHECK(sch.resident_bytes() == bytes - (x.admitted ? x.bytes : 0), "bytes after cancel");
+                CHECK(sch.find(id) == nullptr && sch.cancel(id) == -1, "cancelled request still known");
+                if (!x.admitted) {
+                    auto pos = std::find(submitted.begin() + next_admit, submitted.end(), id);
+                    CHECK(pos != submitted.end(), "cancelled waiting request not queued");
+                    submitted.erase(pos);
+                }
+                x.finished = true;
+                ++finished;
+            }
+        }
         for (long long id : sch.admit()) {
             CHECK(next_admit < submitted.size() && submitted[next_admit] == id, "admission out of order (id %lld)", id);
             ++next_admit;
             t[id].admitted = true;
         }
-        (void)before;
-        CHECK(sch.resident_bytes() <= cap || sch.n_running() + 0 <= 1, "resident %lld over cap %lld with %zu running",
+        CHECK(sch.resident_bytes() <= cap || sch.n_running() <= 1, "resident %lld over cap %lld with %zu running",
               sch.resident_bytes(), cap, sch.n_running());
         iteration_plan p = sch.plan();
         long long tiles = 0;
@@ -95,7 +120,7 @@ int scenario(unsigned seed, long long cap, long long budget, int chunk_rounds) {
                     rounds_here[e.id]++;
                     CHECK(e.steps >= 1 && e.steps <= x.k, "round of %d steps with k=%d", e.steps, x.k);
                     CHECK(e.src == x.cur, "request %lld reads buffer %d, state is in %d", e.id, e.src, x.cur);
-                    CHECK(e.tpar == (x.done & 1), "request %lld step parity", e.id);
+                    CHECK(e.tpar == ((x.t0 + x.done) & 1), "request %lld step parity", e.id);
                     x.cur ^= 1;
                     x.done += e.steps;
                     x.rounds++;

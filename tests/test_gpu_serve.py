@@ -210,3 +210,50 @@ def test_server_rejects_bad_requests(cuda):
         with pytest.raises(lib.CellatoError):
             srv.release(12345)
         assert srv.iterate() == 0
+
+
+def test_server_snapshot_cancel_resume(cuda, oracle):
+    """Preemption without recomputation: requests are advanced part-way, then
+    checkpointed (planes + steps done + next step number) and cancelled, and
+    resumed on a second server from the snapshot with the steps left.  The
+    rules whose steps alternate (traffic, critters' Margolus phase) are among
+    them and resume from odd step numbers.  Results equal the uninterrupted
+    run alone; a snapshot of a request that keeps running leaves its result
+    unchanged."""
+    from cellato_b200.serve import Server
+    layout, W = 1, 64
+    ks = {r: 3 for r in range(10)}      # odd k: snapshots fall on odd step numbers
+    reqs = [(9, 128, 64, 40), (8, 192, 48, 31), (3, 256, 64, 25), (6, 64, 32, 17), (2, 128, 128, 45),
+            (0, 64, 64, 9)]
+    with Server(layout, W, chunk_rounds=1, k_per_rule=ks) as a, Server(layout, W, k_per_rule=ks) as b:
+        ids = []
+        for i, (r, X, Y, steps) in enumerate(reqs):
+            th = inputs.thresholds(inputs.REFERENCE_DENSITY[RULES[r]])
+            ids.append(a.submit_random(r, X, Y, steps, 500 + i, thresholds=th, keep=True))
+        a.iterate()                     # one round of 3 steps each
+        resumed, kept_running = {}, None
+        for i, rid in enumerate(ids):
+            r, X, Y, steps = reqs[i]
+            nb = inputs.PLANES[r]
+            planes, done, nxt = a.snapshot(rid, nb, X, Y)
+            assert nxt == done and 0 < done < steps, (i, done, nxt)
+            if i == len(ids) - 1:
+                kept_running = rid   # this one is checkpointed but left to run on
+                continue
+            a.cancel(rid)
+            resumed[b.submit_planes(r, X, Y, steps - done, list(planes), keep=True, t0=nxt)] = i
+        results = {res["id"]: res for res in b.run_until_idle()}
+        results.update({res["id"]: res for res in a.run_until_idle()})
+        for rid, i in list(resumed.items()) + [(kept_running, len(ids) - 1)]:
+            r, X, Y, steps = reqs[i]
+            srv = a if rid == kept_running else b
+            nb = inputs.PLANES[r]
+            got = lib.download_planes(nb, srv.planes(rid, nb), X * Y // 8)
+            th = inputs.thresholds(inputs.REFERENCE_DENSITY[RULES[r]])
+            init, ref, ref_sum = alone(r, layout, W, X, Y, steps, ks[r], 500 + i, th)
+            assert np.array_equal(got, ref), (i, RULES[r])
+            assert results[rid]["checksum"] == ref_sum, i
+            cells = oracle.unpack(layout, W, nb, init, X, Y)
+            assert np.array_equal(oracle.unpack(layout, W, nb, got, X, Y), oracle.run(r, cells, steps)), i
+        with pytest.raises(lib.CellatoError):
+            a.snapshot(ids[0], 1, 128, 64)    # cancelled: nothing held
