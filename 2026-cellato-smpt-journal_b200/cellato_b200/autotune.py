@@ -17,8 +17,9 @@ import threading
 
 from . import lib
 
-DEFAULT_CANDIDATES = (("simple_register", 1), ("simple_stream", 1), ("temporal", 2),
-                      ("temporal", 4), ("temporal", 6), ("temporal", 8), ("temporal", 12), ("temporal", 16))
+# (mode, k[, tile_rows]); tile_rows 0 = the library's default height for k
+DEFAULT_CANDIDATES = (("simple_register", 1), ("simple_stream", 1), ("temporal", 2)) + tuple(
+    ("temporal", k, th) for k in (4, 6, 8, 12, 16) for th in (0, 96, 128, 160, 192))
 _VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2}
 
 _lock = threading.Lock()
@@ -36,7 +37,7 @@ def cache_path() -> str:
 
 
 def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
-    return f"{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+    return f"v2/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
 
 
 def _load_file() -> dict:
@@ -75,7 +76,8 @@ def run(choice: dict, rule: int, layout: int, word_bits: int, planes_a, planes_b
 
 def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, candidates=DEFAULT_CANDIDATES,
          burst_steps: int = 48, use_cache: bool = True) -> dict:
-    """Measure each candidate on (planes_a, planes_b) and return the fastest.
+    """Measure each candidate (mode, k[, tile_rows]) on (planes_a, planes_b) and
+    return the fastest.
 
     The planes are used as scratch: their content after tuning is some
     evolution of the input.  Returns {"mode", "k", "tile_rows", "ns_per_cell_step"}.
@@ -95,8 +97,12 @@ def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, 
                 return disk
     best = None
     stream = torch.cuda.current_stream().cuda_stream
-    for mode, k in candidates:
-        choice = {"mode": mode, "k": k, "tile_rows": 0}
+    for cand in candidates:
+        mode, k = cand[0], cand[1]
+        th = cand[2] if len(cand) > 2 else 0
+        if th and th - 2 * ((k + 7) // 8 * 8) < 8:
+            continue  # the halos would leave no interior
+        choice = {"mode": mode, "k": k, "tile_rows": th}
         steps = max(burst_steps, 2 * k) // k * k
         try:
             run(choice, rule, layout, word_bits, planes_a, planes_b, X, Y, 0, k, stream)  # warm-up

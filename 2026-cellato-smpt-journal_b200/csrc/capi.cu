@@ -90,13 +90,18 @@ int max_optin_smem() {
     return v;
 }
 
-// Default tile height: the tallest tile that still lets two CTAs share an SM.
-int default_tile_rows(const rule_ops* ops, int R) {
+// Default tile height for k fused steps: 128 interior rows plus the two halos
+// (HY = ceil(k/R)*R rows each), at most what still lets two CTAs share an SM.
+// Taller tiles waste less on halos but leave fewer CTAs for the 148 SMs and
+// fewer resident warps per SM; measured on B200 at 16384^2 over the ten rules,
+// this height is within a few percent of the best single height per rule.
+int default_tile_rows(const rule_ops* ops, int R, int k) {
     const int row_bytes = ops->planes * 32 * ops->temporal_words_per_lane * 4;
-    int rows = (113 * 1024) / row_bytes;
     const int q = std::max(ops->temporal_warps, R);
-    rows = std::min(rows, 512) / q * q;
-    return rows;
+    const int HY = (std::max(1, k) + R - 1) / R * R;
+    const int two_per_sm = (113 * 1024) / row_bytes / q * q;
+    const int want = (2 * HY + 128 + q - 1) / q * q;
+    return std::min(want, std::max(two_per_sm, (2 * HY + q) / q * q));
 }
 
 }  // namespace cellato::b200::capi
@@ -257,7 +262,7 @@ int cellato_run_temporal(int rule, int layout, int word_bits, void* const* plane
     const int L = internal_layout(layout, word_bits);
     const int R = band_height(layout, word_bits);
     const int q = std::max(ops->temporal_warps, R);
-    const int TH = tile_rows > 0 ? tile_rows : default_tile_rows(ops, R);
+    const int TH = tile_rows > 0 ? tile_rows : default_tile_rows(ops, R, k);
     if (TH % q != 0)
         return fail(CELLATO_EINVAL, "temporal tile rows %d must be a multiple of %d", TH, q);
     const int row_bytes = ops->planes * 32 * ops->temporal_words_per_lane * 4;

@@ -705,6 +705,20 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
         }
         write_row(r, o);
     };
+    // Evaluation and in-place write of row r from the three feature rows.
+    auto eval_row = [&](int r, int gy, const feat (&fu)[V], const feat (&fm)[V], const feat (&fd)[V],
+                        auto tp_tag) {
+        constexpr int TP = decltype(tp_tag)::value;
+        word o[NB][V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            word ov[NB];
+            Net::template eval<TP>(fu[v], fm[v], fd[v], gy & 1, ov);
+#pragma unroll
+            for (int p = 0; p < NB; ++p) o[p][v] = ov[p];
+        }
+        write_row(r, o);
+    };
 
     auto step = [&](int t, auto tp_tag) {
         const int lo = max(rw0, t);
@@ -728,13 +742,32 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
             if (gy < 0) gy += Y;
             auto next_gy = [&](int g) { return g + 1 == Y ? 0 : g + 1; };
             int r = lo;
-            // three rows per trip: the feature buffers rotate by name, not by copy
+            // Three rows per trip; the feature buffers rotate by name, not by
+            // copy.  The trip's three input rows (r+1 .. r+3, the last one the
+            // saved row below the band when r+3 == hi) are read before any of
+            // its in-place writes: they are the old values the writes replace,
+            // and issuing them together keeps one shared-memory latency per
+            // trip instead of one per row, with three rows of independent work.
             for (; r + 3 <= hi; r += 3) {
-                row_body(r, hi, gy, fa, fb, fc, botC, tp_tag);
+                word C1[NB][V], C2[NB][V], C3[NB][V];
+                read_row(r + 1, C1);
+                read_row(r + 2, C2);
+                if (r + 3 < hi) {
+                    read_row(r + 3, C3);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < NB; ++p)
+#pragma unroll
+                        for (int v = 0; v < V; ++v) C3[p][v] = botC[p][v];
+                }
+                feats(C1, fc);
+                eval_row(r, gy, fa, fb, fc, tp_tag);
                 gy = next_gy(gy);
-                row_body(r + 1, hi, gy, fb, fc, fa, botC, tp_tag);
+                feats(C2, fa);
+                eval_row(r + 1, gy, fb, fc, fa, tp_tag);
                 gy = next_gy(gy);
-                row_body(r + 2, hi, gy, fc, fa, fb, botC, tp_tag);
+                feats(C3, fb);
+                eval_row(r + 2, gy, fc, fa, fb, tp_tag);
                 gy = next_gy(gy);
             }
             if (r < hi) {
