@@ -17,9 +17,10 @@ import threading
 
 from . import lib
 
-# (mode, k[, tile_rows]); tile_rows 0 = the library's default height for k
+# (mode, k[, tile_rows[, row loop]]); tile_rows 0 = the library's default height
+# for k; row loop as cellato_set_temporal_variant (0 = default)
 DEFAULT_CANDIDATES = (("simple_register", 1), ("simple_stream", 1), ("temporal", 2)) + tuple(
-    ("temporal", k, th) for k in (4, 6, 8, 12, 16) for th in (0, 96, 128, 160, 192))
+    ("temporal", k, th, loop) for k in (4, 6, 8, 12, 16) for th in (0, 96, 128, 160, 192) for loop in (1, 2))
 _VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2}
 
 _lock = threading.Lock()
@@ -37,7 +38,7 @@ def cache_path() -> str:
 
 
 def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
-    return f"v2/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+    return f"v3/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
 
 
 def _load_file() -> dict:
@@ -70,8 +71,12 @@ def run(choice: dict, rule: int, layout: int, word_bits: int, planes_a, planes_b
             return lib.run_simple(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, stream)
         finally:
             lib.set_simple_variant(0)
-    return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
-                            choice.get("tile_rows", 0), stream)
+    lib.set_temporal_variant(choice.get("loop", 0))
+    try:
+        return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
+                                choice.get("tile_rows", 0), stream)
+    finally:
+        lib.set_temporal_variant(0)
 
 
 def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, candidates=DEFAULT_CANDIDATES,
@@ -100,9 +105,10 @@ def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, 
     for cand in candidates:
         mode, k = cand[0], cand[1]
         th = cand[2] if len(cand) > 2 else 0
+        loop = cand[3] if len(cand) > 3 else 0
         if th and th - 2 * ((k + 7) // 8 * 8) < 8:
             continue  # the halos would leave no interior
-        choice = {"mode": mode, "k": k, "tile_rows": th}
+        choice = {"mode": mode, "k": k, "tile_rows": th, "loop": loop}
         steps = max(burst_steps, 2 * k) // k * k
         try:
             run(choice, rule, layout, word_bits, planes_a, planes_b, X, Y, 0, k, stream)  # warm-up

@@ -27,7 +27,7 @@ EXPORTED = [
     "cellato_planes_alloc", "cellato_planes_free", "cellato_planes_upload", "cellato_planes_download",
     "cellato_pack_cells", "cellato_unpack_cells",
     "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
-    "cellato_device_wait_timeouts", "cellato_set_simple_variant",
+    "cellato_device_wait_timeouts", "cellato_set_simple_variant", "cellato_set_temporal_variant",
     "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
     "cellato_batch_destroy", "cellato_batch_run_noalloc",
     "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random",
@@ -180,6 +180,11 @@ def unpack_cells(layout: int, word_bits: int, nb: int, planes, X: int, Y: int, c
 def set_simple_variant(variant: int) -> None:
     """0 automatic, 1 register-band kernel, 2 bulk-copy streaming kernel (linear layout)."""
     check(load().cellato_set_simple_variant(variant))
+
+
+def set_temporal_variant(variant: int) -> None:
+    """0 automatic, 1 row-by-row reads, 2 hoisted reads per three-row trip (temporal kernel)."""
+    check(load().cellato_set_temporal_variant(variant))
 
 
 def device_wait_timeouts() -> int:

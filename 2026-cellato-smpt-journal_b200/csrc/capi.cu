@@ -227,6 +227,12 @@ int cellato_set_simple_variant(int variant) {
     return CELLATO_OK;
 }
 
+int cellato_set_temporal_variant(int variant) {
+    if (variant < 0 || variant > 2) return fail(CELLATO_EINVAL, "temporal kernel variant must be 0, 1 or 2");
+    temporal_variant() = variant;
+    return CELLATO_OK;
+}
+
 int cellato_device_wait_timeouts(unsigned* count) {
     if (!count) return fail(CELLATO_EINVAL, "count must not be NULL");
     *count = 0;

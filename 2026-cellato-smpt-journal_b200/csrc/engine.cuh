@@ -597,7 +597,11 @@ __global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, p
 // two rows bordering a band belong to other warps: they are read before the
 // first barrier of the step and every write happens after it.  At step t only
 // rows t .. TH-1-t are computed (the valid region shrinks by one row per step).
-template <class Net, int NB, int LAYOUT, int V, int WARPS>
+// HOIST selects the row loop: true reads the three input rows of each 3-row
+// trip before the trip's writes; false reads each row just before the row
+// above it is evaluated.  Both compute the same values; which is faster
+// depends on the rule's register use and the occupancy (the autotuner picks).
+template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST = true>
 __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                                               int TH, int HY, int bx, int by) {
     constexpr int R = band_rows<LAYOUT>();
@@ -743,23 +747,28 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
             auto next_gy = [&](int g) { return g + 1 == Y ? 0 : g + 1; };
             int r = lo;
             // Three rows per trip; the feature buffers rotate by name, not by
-            // copy.  The trip's three input rows (r+1 .. r+3, the last one the
-            // saved row below the band when r+3 == hi) are read before any of
-            // its in-place writes: they are the old values the writes replace,
+            // copy.  The trip's three input rows (r+1 .. r+3) are read before
+            // any of its in-place writes: they are the old values the writes replace,
             // and issuing them together keeps one shared-memory latency per
             // trip instead of one per row, with three rows of independent work.
-            for (; r + 3 <= hi; r += 3) {
+            if constexpr (!HOIST) {
+                for (; r + 3 <= hi; r += 3) {
+                    row_body(r, hi, gy, fa, fb, fc, botC, tp_tag);
+                    gy = next_gy(gy);
+                    row_body(r + 1, hi, gy, fb, fc, fa, botC, tp_tag);
+                    gy = next_gy(gy);
+                    row_body(r + 2, hi, gy, fc, fa, fb, botC, tp_tag);
+                    gy = next_gy(gy);
+                }
+            }
+            // (Trips stop while r+3 is still inside the band, so all three
+            // reads come from shared memory; the band's last rows go through
+            // row_body below, which takes the saved row when it needs it.)
+            for (; HOIST && r + 3 < hi; r += 3) {
                 word C1[NB][V], C2[NB][V], C3[NB][V];
                 read_row(r + 1, C1);
                 read_row(r + 2, C2);
-                if (r + 3 < hi) {
-                    read_row(r + 3, C3);
-                } else {
-#pragma unroll
-                    for (int p = 0; p < NB; ++p)
-#pragma unroll
-                        for (int v = 0; v < V; ++v) C3[p][v] = botC[p][v];
-                }
+                read_row(r + 3, C3);
                 feats(C1, fc);
                 eval_row(r, gy, fa, fb, fc, tp_tag);
                 gy = next_gy(gy);
@@ -773,7 +782,11 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
             if (r < hi) {
                 row_body(r, hi, gy, fa, fb, fc, botC, tp_tag);
                 gy = next_gy(gy);
-                if (r + 1 < hi) row_body(r + 1, hi, gy, fb, fc, fa, botC, tp_tag);
+                if (r + 1 < hi) {
+                    row_body(r + 1, hi, gy, fb, fc, fa, botC, tp_tag);
+                    gy = next_gy(gy);
+                    if (r + 2 < hi) row_body(r + 2, hi, gy, fc, fa, fb, botC, tp_tag);
+                }
             }
         }
         __syncthreads();
@@ -806,10 +819,10 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
     }
 }
 
-template <class Net, int NB, int LAYOUT, int V, int WARPS>
+template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST>
 __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plane_set out, int Xw, int Y, int t0,
                                                               int k, int TH, int HY) {
-    temporal_tile<Net, NB, LAYOUT, V, WARPS>(in, out, Xw, Y, t0, k, TH, HY, blockIdx.x, blockIdx.y);
+    temporal_tile<Net, NB, LAYOUT, V, WARPS, HOIST>(in, out, Xw, Y, t0, k, TH, HY, blockIdx.x, blockIdx.y);
 }
 
 // ======================================================= batched temporal kernel

@@ -22,6 +22,13 @@ inline int& simple_variant() {
     return v;
 }
 
+// Row loop of the temporal kernel: 0 = the library's choice (hoisted reads),
+// 1 = row by row, 2 = hoisted reads of each 3-row trip.  Process-wide.
+inline int& temporal_variant() {
+    static int v = 0;
+    return v;
+}
+
 struct rule_ops {
     const char* name;
     int planes;  // needed_bits
@@ -145,7 +152,8 @@ struct rule_kernels {
     static cudaError_t temporal_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                                        int TH, int HY, cudaStream_t s) {
         constexpr int V = TEMPORAL_V;
-        auto kern = temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS>;
+        auto kern = temporal_variant() == 1 ? temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, false>
+                                            : temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, true>;
         const size_t smem = (size_t)NB * TH * 32 * V * sizeof(word);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

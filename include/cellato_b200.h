@@ -151,6 +151,14 @@ int cellato_run_temporal(int rule, int layout, int word_bits, void* const* plane
  * reference (one simple kernel). */
 int cellato_set_simple_variant(int variant);
 
+/* Selects the row loop of the temporal kernel (cellato_run_temporal): 0 =
+ * automatic, 1 = each row read just before the row above it is evaluated, 2 =
+ * the input rows of each three-row trip read before the trip's in-place writes.
+ * Same results; the speed depends on the rule.  Process-wide, not synchronised
+ * with concurrent launches; the autotuner sweeps it.  No counterpart in the
+ * reference (one temporal kernel). */
+int cellato_set_temporal_variant(int variant);
+
 /* Reads and clears the number of bounded device-side waits (mbarrier waits of
  * the streaming single-step kernel) that gave up since the last call; returns
  * CELLATO_ETIMEDOUT when it is non-zero.  Synchronises the device.  No

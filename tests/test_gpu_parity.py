@@ -49,6 +49,21 @@ def test_temporal_small_golden(cuda, oracle, golden_small, layout, W, k):
         assert np.array_equal(out, cout), (case["key"], case["rule"], k, int((out != cout).sum()))
 
 
+@pytest.mark.parametrize("loop", [1, 2])
+@pytest.mark.parametrize("k", [3, 8])
+@pytest.mark.parametrize("layout,W", LAYOUTS)
+def test_temporal_row_loops(cuda, oracle, golden_small, layout, W, k, loop):
+    """Both row loops of the temporal kernel (cellato_set_temporal_variant)."""
+    lib.set_temporal_variant(loop)
+    try:
+        for case, cin, cout in golden_small:
+            r = RULES.index(case["rule"])
+            out = run_gpu(oracle, r, layout, W, cin, case["steps"], mode="temporal", k=k, tile_rows=48)
+            assert np.array_equal(out, cout), (case["key"], case["rule"], k, loop)
+    finally:
+        lib.set_temporal_variant(0)
+
+
 @pytest.mark.parametrize("mode,k", [("simple", 1), ("temporal", 3), ("temporal", 8)])
 @pytest.mark.parametrize("t0", [1, 2, 7])
 def test_step_parity_offsets(cuda, oracle, mode, k, t0):
