@@ -19,7 +19,12 @@ from . import lib
 
 # (mode, k[, tile_rows[, row loop]]); tile_rows 0 = the library's default height
 # for k; row loop as cellato_set_temporal_variant (0 = default)
-DEFAULT_CANDIDATES = (("simple_register", 1), ("simple_stream", 1), ("temporal", 2)) + tuple(
+# Single-step candidates: the two single-step kernels and the temporal kernel at
+# k = 1 (one step per launch through a shared-memory tile), which for rules with
+# many planes or long networks reaches more of the HBM roofline.
+SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1)) + tuple(
+    ("temporal", 1, th, loop) for th in (0, 96, 128) for loop in (1, 2))
+DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2),) + tuple(
     ("temporal", k, th, loop) for k in (4, 6, 8, 12, 16) for th in (0, 96, 128, 160, 192) for loop in (1, 2))
 _VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2}
 
@@ -38,7 +43,7 @@ def cache_path() -> str:
 
 
 def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
-    return f"v3/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+    return f"v4/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
 
 
 def _load_file() -> dict:

@@ -46,8 +46,8 @@ CPU_SAMPLE_SIZE = 2048
 # DRAM bytes (read + write) per launch measured by one ncu capture of the same
 # configuration (summaries in profiles/); keyed by (rule, mode, k, size).
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 8, 16384): (83.40e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md"),
-    ("excitable", "temporal", 16, 16384): (152.92e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
+    ("wire", "temporal", 8, 16384): (85.10e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md"),
+    ("excitable", "temporal", 16, 16384): (154.04e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
 }
 
 
@@ -57,11 +57,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--size", type=int, default=SIZE)
-    ap.add_argument("--ca-steps", type=int, default=CA_STEPS)
+    ap.add_argument("--size", type=int, default=None, help="grid side (default: the workload's)")
+    ap.add_argument("--ca-steps", type=int, default=None, help="steps per automaton (default: the workload's)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="config2", choices=["config2", "batched", "served"],
+    ap.add_argument("--choice", default="", help="pin the traverser per automaton instead of autotuning, "
+                                                 "e.g. wire=temporal:8:128:1,excitable=temporal:16:0:2")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "batched", "served"],
                     help="config2: WireWorld + Greenberg-Hastings 16384^2 x 1000 steps (default); "
+                         "config3: cyclic + HPP fluid 32768^2 x 256 steps on bit_planes, with the single-step "
+                         "kernels' HBM roofline beside the autotuned run; "
                          "batched: many mixed grids in one CUDA-graph launch vs per-grid launches; "
                          "served: a Poisson request stream through the continuous-batching server")
     ap.add_argument("--batch-grids", type=int, default=4096)
@@ -76,7 +80,26 @@ def parse():
     ap.add_argument("--serve-max-steps", type=int, default=10000)
     ap.add_argument("--serve-check-fraction", type=float, default=0.01)
     ap.add_argument("--no-per-grid", action="store_true", help="served: skip the per-grid baseline run")
-    return ap.parse_args()
+    args = ap.parse_args()
+    apply_workload(args)
+    return args
+
+
+# workload -> (automata, side, steps per automaton, layout)
+SINGLE_GRID_WORKLOADS = {
+    "config2": (("wire", "excitable"), SIZE, CA_STEPS, 1),
+    "config3": (("cyclic", "fluid"), 32768, 256, 0),
+}
+
+
+def apply_workload(args) -> None:
+    """Sets the automata, sizes and layout of a single-grid workload."""
+    global AUTOMATA, LAYOUT
+    automata, side, steps, layout = SINGLE_GRID_WORKLOADS.get(args.workload, SINGLE_GRID_WORKLOADS["config2"])
+    if args.workload in SINGLE_GRID_WORKLOADS:
+        AUTOMATA, LAYOUT = automata, layout
+    args.size = args.size or side
+    args.ca_steps = args.ca_steps or steps
 
 
 def host_threads() -> int:
@@ -222,12 +245,38 @@ def reference_arm(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def parse_choices(text: str) -> dict:
+    """--choice wire=temporal:8:128:1,excitable=temporal:16:0:2 (mode:k:tile_rows:loop)
+    or <automaton>=simple_register / simple_stream: pins the traverser per automaton."""
+    out = {}
+    for item in filter(None, (text or "").split(",")):
+        name, spec = item.split("=")
+        f = spec.split(":")
+        if f[0] == "temporal":
+            out[name] = {"mode": "temporal", "k": int(f[1]), "tile_rows": int(f[2]) if len(f) > 2 else 0,
+                         "loop": int(f[3]) if len(f) > 3 else 0}
+        else:
+            out[name] = {"mode": f[0], "k": 1, "tile_rows": 0}
+    return out
+
+
+def describe_choice(c: dict) -> str:
+    """The autotuner's choice as text: mode, k, tile rows (0 = default) and row loop."""
+    if c["mode"] != "temporal":
+        return c["mode"]
+    loop = {0: "default", 1: "row-by-row", 2: "hoisted"}[c.get("loop", 0)]
+    return f"temporal k={c['k']} tile_rows={c.get('tile_rows', 0)} loop={loop}"
+
+
 def workload_config(args, extra=None):
-    c = {"workload": f"wire+excitable {args.size}x{args.size} tiled_bit_planes W64, {args.ca_steps} steps each, "
-                     f"traverser autotuned (simple | temporal k)",
+    from cellato_b200 import inputs
+    layout = "tiled_bit_planes" if LAYOUT == 1 else "bit_planes"
+    mib = [2 * inputs.PLANES[inputs.RULE_ID[a]] * args.size * args.size // 8 >> 20 for a in AUTOMATA]
+    c = {"workload": f"{'+'.join(AUTOMATA)} {args.size}x{args.size} {layout} W{WORD_BITS}, {args.ca_steps} steps "
+                     f"each, traverser autotuned (simple | temporal k)",
          "automata": list(AUTOMATA), "x_size": args.size, "y_size": args.size, "ca_steps_per_step": args.ca_steps,
-         "layout": "tiled_bit_planes", "word_size": WORD_BITS,
-         "l2": "inputs larger than L2 (ping-pong planes 128 MiB + 192 MiB), no flush"}
+         "layout": layout, "word_size": WORD_BITS,
+         "l2": f"inputs larger than L2 (ping-pong planes {' MiB + '.join(str(m) for m in mib)} MiB), no flush"}
     if extra:
         c.update(extra)
     return c
@@ -258,9 +307,11 @@ def our_arm(args, rank: int, world: int):
         grids[a] = {"rule": r, "nb": nb, "a": pa, "b": pb, "init": init}
     torch.cuda.synchronize()
 
-    # autotune per automaton (on scratch copies of the planes)
+    # autotune per automaton (on scratch copies of the planes), unless pinned
+    pinned = parse_choices(args.choice)
     for a, g in grids.items():
-        choice = autotune.tune(g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, use_cache=False)
+        choice = pinned.get(a) or autotune.tune(g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y,
+                                                use_cache=False)
         g["choice"] = choice
         g["a"].buf.copy_(g["init"].buf)
     torch.cuda.synchronize()
@@ -352,8 +403,29 @@ def our_arm(args, rank: int, world: int):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
     e2e_value = cells_per_step * args.steps * world / (e2e_ms * 1e-3) / 1e9
 
-    # ---- roofline of the dominant kernel (the automaton with the most time)
     peaks = measured_peaks()
+    # ---- the best single-step kernel of each automaton against the HBM roofline
+    # (one step per launch: read and write every plane once)
+    single = {}
+    for a, g in grids.items():
+        c1 = autotune.tune(g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y,
+                           candidates=autotune.SINGLE_STEP_CANDIDATES, use_cache=False)
+        g["a"].buf.copy_(g["init"].buf)
+        n1 = 16
+        autotune.run(c1, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, 2, sp)
+        e0.record(stream)
+        autotune.run(c1, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, n1, sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms1 = e0.elapsed_time(e1) / n1
+        gbs = 2 * g["nb"] * g["init"].plane_bytes / (ms1 * 1e-3) / 1e9
+        single[a] = {"kernel": describe_choice(c1), "ms_per_step": round(ms1, 4), "achieved_gbs": round(gbs, 1),
+                     "frac": round(gbs / peaks["hbm_gbs"], 4),
+                     "gcups": round(X * Y / (ms1 * 1e-3) / 1e9, 1)}
+        g["a"].buf.copy_(g["init"].buf)
+    torch.cuda.synchronize()
+
+    # ---- roofline of the dominant kernel (the automaton with the most time)
     dom = max(AUTOMATA, key=lambda a: sum(per[a]))
     g = grids[dom]
     n_dom = launches(g) * args.steps
@@ -388,14 +460,13 @@ def our_arm(args, rank: int, world: int):
         "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded i.i.d. grids)",
         "config": workload_config(args, extra={
-            "traverser": {a: grids[a]["choice"]["mode"] + (f" k={grids[a]['choice']['k']}"
-                                                           if grids[a]["choice"]["mode"] == "temporal" else "")
-                          for a in AUTOMATA},
+            "traverser": {a: describe_choice(grids[a]["choice"]) for a in AUTOMATA},
             "parallelism": f"replicas x{world}"}),
         "per_automaton_gcups": {a: round(v, 1) for a, v in per_gcups.items()},
         "e2e": {"value": round(e2e_value, 1), "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": n_launch,
         "roofline": roof,
+        "single_step_roofline": {"peak_gbs": peaks["hbm_gbs"], "peak_source": peaks["source"], **single},
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
     }
