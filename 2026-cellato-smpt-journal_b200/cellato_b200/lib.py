@@ -30,7 +30,7 @@ EXPORTED = [
     "cellato_device_wait_timeouts", "cellato_set_simple_variant", "cellato_set_temporal_variant",
     "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
     "cellato_batch_destroy", "cellato_batch_run_noalloc",
-    "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random",
+    "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random", "cellato_diff_cells",
     "cellato_server_create", "cellato_server_submit_random", "cellato_server_submit_planes",
     "cellato_server_iterate", "cellato_server_poll", "cellato_server_planes", "cellato_server_release",
     "cellato_server_stats_get", "cellato_server_destroy", "cellato_server_submit_resume",
@@ -106,6 +106,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     u32p = ctypes.POINTER(ctypes.c_uint32)
     ll = ctypes.c_longlong
     lib.cellato_checksum.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
+    lib.cellato_diff_cells.argtypes = [i, _PP, _PP, ctypes.c_size_t, _vp, _vp]
     lib.cellato_rule_state_value.argtypes = [i, i, ctypes.POINTER(ll)]
     lib.cellato_fill_random.argtypes = [i, i, i, _PP, i, i, ctypes.c_ulonglong, u32p, i, _vp]
     lib.cellato_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]
@@ -235,3 +236,9 @@ def download_planes(nb: int, dev_ptrs, plane_bytes: int, stream: int = 0):
     host = ptr_array([out[p].ctypes.data for p in range(nb)])
     check(load().cellato_planes_download(nb, host, ptr_array(dev_ptrs), plane_bytes, stream))
     return out
+
+
+def diff_cells(nb: int, planes_a, planes_b, plane_bytes: int, count_ptr: int, stream: int = 0) -> None:
+    """Number of differing cells between two grids of the same layout, into one
+    uint64 of device memory at count_ptr."""
+    check(load().cellato_diff_cells(nb, ptr_array(planes_a), ptr_array(planes_b), plane_bytes, count_ptr, stream))

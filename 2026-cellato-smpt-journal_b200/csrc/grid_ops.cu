@@ -1,5 +1,6 @@
-// Whole-grid operations on bit planes: the 4 x 4 tile checksum and a seeded
-// random initial state, both computed where the planes live.
+// Whole-grid operations on bit planes: the 4 x 4 tile checksum, a full-grid
+// diff (count of differing cells) and a seeded random initial state, all
+// computed where the planes live.
 //
 // Checksum.  The reference reduces a grid to sixteen numbers -- the sums of
 // the cells' state values over a 4 x 4 partition into tiles of ceil(X/4) x
@@ -26,6 +27,7 @@
 // single-grid runs of the same planes.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 
@@ -178,6 +180,33 @@ __global__ void __launch_bounds__(OPS_WARPS * 32) fill_random_kernel(int X, int 
     }
 }
 
+// Cells that differ between two grids of the same layout: a cell is one bit
+// position in every plane, so per word the differing cells are the OR over the
+// planes of a ^ b.  128-bit loads, grid-stride; one atomic per warp.
+__global__ void __launch_bounds__(256) diff_kernel(plane_set a, plane_set b, int nb, long long n_words,
+                                                   unsigned long long* __restrict__ out) {
+    const long long n4 = n_words / 4;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    unsigned long long local = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        uint4 acc = make_uint4(0, 0, 0, 0);
+        for (int p = 0; p < nb; ++p) {
+            const uint4 x = reinterpret_cast<const uint4*>(a.p[p])[i];
+            const uint4 y = reinterpret_cast<const uint4*>(b.p[p])[i];
+            acc.x |= x.x ^ y.x, acc.y |= x.y ^ y.y, acc.z |= x.z ^ y.z, acc.w |= x.w ^ y.w;
+        }
+        local += __popc(acc.x) + __popc(acc.y) + __popc(acc.z) + __popc(acc.w);
+    }
+    for (long long i = 4 * n4 + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_words; i += stride) {
+        word acc = 0;
+        for (int p = 0; p < nb; ++p) acc |= a.p[p][i] ^ b.p[p][i];
+        local += __popc(acc);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
+
 // Moebius transform of the value table over the nb index bits.
 int make_terms(const rule_ops* ops, checksum_terms& terms) {
     const int nb = ops->planes, n = 1 << nb;
@@ -316,6 +345,26 @@ int cellato_fill_random(int layout, int word_bits, int nb, void* const* planes, 
     if (int rc = planes_of(nb, planes, ps)) return rc;
     return enqueue_fill_random(layout, word_bits, nb, ps, x_cells, y_cells, seed, thresholds, n_thresholds,
                                reinterpret_cast<cudaStream_t>(stream));
+}
+
+int cellato_diff_cells(int nb, const void* const* planes_a, const void* const* planes_b, size_t plane_bytes,
+                       unsigned long long* count, cellato_stream_t stream) {
+    if (!count) return fail(CELLATO_EINVAL, "count must not be NULL");
+    if (plane_bytes % 4) return fail(CELLATO_EINVAL, "plane bytes %zu are not whole 32-bit words", plane_bytes);
+    plane_set pa, pb;
+    if (int rc = planes_of(nb, const_cast<void* const*>(planes_a), pa)) return rc;
+    if (int rc = planes_of(nb, const_cast<void* const*>(planes_b), pb)) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync (diff)");
+    const long long n_words = (long long)(plane_bytes / 4);
+    if (n_words > 0) {
+        const long long want = (n_words / 4 + 255) / 256;
+        const int blocks = (int)std::max(1LL, std::min(want, 148LL * 8));
+        diff_kernel<<<blocks, 256, 0, s>>>(pa, pb, nb, n_words, count);
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? CELLATO_OK : cuda_fail(e, "diff launch");
 }
 
 int cellato_rule_state_value(int rule, int index, long long* value) {

@@ -286,7 +286,7 @@ def workload_config(args, extra=None):
 def our_arm(args, rank: int, world: int):
     import numpy as np
     import torch
-    from cellato_b200 import autotune, inputs, lib
+    from cellato_b200 import autotune, inputs, lib, replicas
     from cellato_b200.device import DevicePlanes
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
@@ -333,7 +333,7 @@ def our_arm(args, rank: int, world: int):
 
     def barrier():
         if world > 1:
-            torch.distributed.barrier()
+            replicas.barrier()
 
     t0 = 0
     for _ in range(args.warmup):
@@ -764,23 +764,14 @@ def measured_peaks():
 
 
 def max_over_ranks(ms: float, world: int) -> float:
-    if world <= 1:
-        return ms
-    import torch
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
+    from cellato_b200 import replicas
+    return replicas.max_over_ranks(ms) if world > 1 else ms
 
 
 def main():
     args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from cellato_b200 import replicas
+    rank, world = replicas.init(timeout_s=120)
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)
@@ -791,9 +782,7 @@ def main():
         else:
             our_arm(args, rank, world)
     finally:
-        if world > 1:
-            import torch
-            torch.distributed.destroy_process_group()
+        replicas.shutdown()
 
 
 if __name__ == "__main__":

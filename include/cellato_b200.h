@@ -238,6 +238,15 @@ int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits);
 int cellato_checksum(int rule, int layout, int word_bits, const void* const* planes, int x_cells, int y_cells,
                      unsigned long long* sums, cellato_stream_t stream);
 
+/* Full-grid diff: the number of cells whose state differs between two grids
+ * of nb planes of plane_bytes each, in the same layout and word size (a cell
+ * is the same bit position in every plane of either grid).  *count: one uint64
+ * in DEVICE memory, overwritten (stream-ordered, no allocation).  Replaces
+ * comparing two grids cell by cell after to_standard on the host (as the
+ * reference's tests do, include/tests/bit_planes_grid.hpp:135-476). */
+int cellato_diff_cells(int nb, const void* const* planes_a, const void* const* planes_b, size_t plane_bytes,
+                       unsigned long long* count, cellato_stream_t stream);
+
 /* State value of dictionary index `index` of a rule (index_to_state,
  * include/memory/state_dictionary.hpp:10-70). */
 int cellato_rule_state_value(int rule, int index, long long* value);

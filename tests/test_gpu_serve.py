@@ -257,3 +257,30 @@ def test_server_snapshot_cancel_resume(cuda, oracle):
             assert np.array_equal(oracle.unpack(layout, W, nb, got, X, Y), oracle.run(r, cells, steps)), i
         with pytest.raises(lib.CellatoError):
             a.snapshot(ids[0], 1, 128, 64)    # cancelled: nothing held
+
+
+def test_diff_cells(cuda, oracle):
+    """Full-grid diff against numpy on unpacked cells, for each layout and plane
+    count, on grids whose plane size is and is not a multiple of 16 bytes."""
+    import torch
+    from cellato_b200.device import DevicePlanes
+    rng = np.random.default_rng(31)
+    for layout, W in LAYOUTS:
+        for r, (X, Y) in [(6, (4096, 512)), (2, (64, 8)), (0, (32, 9)), (7, (96, 40))]:
+            if (layout == 1 and Y % (W // 8)) or (layout == 0 and X % W):
+                continue
+            nb = inputs.PLANES[r]
+            c1 = rng.integers(0, inputs.STATES[r], size=(Y, X), dtype=np.uint8)
+            c2 = c1.copy()
+            flips = rng.random((Y, X)) < 0.01
+            c2[flips] = (c2[flips] + 1) % inputs.STATES[r]
+            a, b = DevicePlanes(nb, X, Y), DevicePlanes(nb, X, Y)
+            a.upload(oracle.pack(layout, W, nb, c1))
+            b.upload(oracle.pack(layout, W, nb, c2))
+            out = torch.zeros(1, dtype=torch.int64, device="cuda")
+            lib.diff_cells(nb, a.ptrs, b.ptrs, X * Y // 8, out.data_ptr())
+            torch.cuda.synchronize()
+            assert int(out.item()) == int((c1 != c2).sum()), (layout, W, RULES[r], X, Y)
+            lib.diff_cells(nb, a.ptrs, a.ptrs, X * Y // 8, out.data_ptr())
+            torch.cuda.synchronize()
+            assert int(out.item()) == 0
