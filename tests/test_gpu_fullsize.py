@@ -1,0 +1,103 @@
+"""Properties at the workloads' full sizes, where the oracle is too slow to run:
+the grids are seeded on the device, and kernels check one another.
+
+* WireWorld and Greenberg-Hastings on 16384 x 16384 (the tiled W=64 workload):
+  temporal runs with the depths, tile heights and row loops the autotuner picks
+  agree with the single-step kernel.  The full-grid diff of the planes is zero
+  and the checksums are equal.
+* The same seeded grid run on the linear and on the tiled layout has the same
+  checksum (the checksum is over cell values, not bytes).
+* Cyclic and HPP fluid on 32768 x 32768 (the bit_planes workload): temporal k=8
+  and the k=1 temporal path agree with the single-step kernel.
+The smaller sizes are pinned to the reference by the golden fixtures; these
+tests pin the large ones to the small-size-verified kernels."""
+import numpy as np
+import pytest
+
+from cellato_b200 import inputs, lib
+
+pytestmark = pytest.mark.gpu
+
+
+def seeded(rule, layout, X, Y, seed):
+    from cellato_b200.device import DevicePlanes
+    nb = inputs.PLANES[rule]
+    a, b = DevicePlanes(nb, X, Y), DevicePlanes(nb, X, Y)
+    lib.fill_random(layout, 64, nb, a.ptrs, X, Y, seed,
+                    inputs.thresholds(inputs.REFERENCE_DENSITY[inputs.RULES[rule]]))
+    return a, b
+
+
+def run(rule, layout, X, Y, steps, seed, mode, k=1, tile_rows=0, loop=0):
+    a, b = seeded(rule, layout, X, Y, seed)
+    lib.set_temporal_variant(loop)
+    try:
+        if mode == "simple":
+            in_b = lib.run_simple(rule, layout, 64, a.ptrs, b.ptrs, X, Y, 0, steps)
+        else:
+            in_b = lib.run_temporal(rule, layout, 64, a.ptrs, b.ptrs, X, Y, 0, steps, k, tile_rows)
+    finally:
+        lib.set_temporal_variant(0)
+    res = b if in_b else a
+    other = a if in_b else b
+    del other
+    return res
+
+
+def diff(nb, p, q):
+    import torch
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    lib.diff_cells(nb, p.ptrs, q.ptrs, p.plane_bytes, out.data_ptr())
+    torch.cuda.synchronize()
+    return int(out.item())
+
+
+def checksum(rule, layout, p, X, Y):
+    import torch
+    sums = torch.zeros(16, dtype=torch.int64, device="cuda")
+    lib.checksum(rule, layout, 64, p.ptrs, X, Y, sums.data_ptr())
+    torch.cuda.synchronize()
+    return sums.cpu().tolist()
+
+
+@pytest.mark.parametrize("rule,k,th,loop", [("wire", 8, 128, 1), ("wire", 16, 0, 2),
+                                            ("excitable", 16, 0, 2), ("excitable", 8, 128, 1)])
+def test_config2_size_temporal_equals_single_step(cuda, rule, k, th, loop):
+    import torch
+    r = lib.rule_id(rule)
+    S, steps = 16384, 48
+    ref = run(r, 1, S, S, steps, 42, "simple")
+    got = run(r, 1, S, S, steps, 42, "temporal", k, th, loop)
+    assert diff(inputs.PLANES[r], ref, got) == 0
+    assert checksum(r, 1, ref, S, S) == checksum(r, 1, got, S, S)
+    del ref, got
+    torch.cuda.empty_cache()
+
+
+def test_config2_size_layouts_agree_on_checksums(cuda):
+    import torch
+    S, steps = 16384, 40
+    for rule in ("wire", "excitable"):
+        r = lib.rule_id(rule)
+        lin = run(r, 0, S, S, steps, 7, "temporal", 8)
+        til = run(r, 1, S, S, steps, 7, "temporal", 8)
+        c = checksum(r, 0, lin, S, S)
+        assert c == checksum(r, 1, til, S, S), rule
+        assert sum(c) > 0
+        del lin, til
+        torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("rule", ["cyclic", "fluid"])
+def test_config3_size_temporal_equals_single_step(cuda, rule):
+    import torch
+    r = lib.rule_id(rule)
+    S, steps = 32768, 24
+    ref = run(r, 0, S, S, steps, 42, "simple")
+    for k, th, loop in ((8, 0, 2), (1, 128, 1)):
+        got = run(r, 0, S, S, steps, 42, "temporal", k, th, loop)
+        assert diff(inputs.PLANES[r], ref, got) == 0, (rule, k)
+        del got
+        torch.cuda.empty_cache()
+    del ref
+    torch.cuda.empty_cache()
