@@ -589,14 +589,16 @@ __global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, p
 // above and below (HY >= k, a multiple of the band height), so after k steps
 // its interior -- words 1 .. 32V-2, rows HY .. TH-HY-1 -- is exact.
 //
-// Steps update the tile in place.  Warps own horizontal bands of the tile
-// (TH / WARPS rows each) and sweep them top-down: the rolling window keeps the
-// old value of the row above in registers, the row below is read before it is
-// overwritten, and horizontal neighbours come from lane shuffles of registers,
-// so no lane ever reads a word another lane writes within a step.  Only the
+// Steps update the tile in place.  At step t only rows t .. TH-1-t are
+// computed (the valid region shrinks by one row per step); they are split into
+// WARPS contiguous bands of equal size (within one row), so the warps stay
+// balanced as the region shrinks.  Each warp sweeps its band top-down: the
+// rolling window keeps the old value of the row above in registers, the row
+// below is read before it is overwritten, and horizontal neighbours come from
+// lane shuffles of registers, so no lane ever reads a word another lane writes
+// within a step.  Only the
 // two rows bordering a band belong to other warps: they are read before the
-// first barrier of the step and every write happens after it.  At step t only
-// rows t .. TH-1-t are computed (the valid region shrinks by one row per step).
+// first barrier of the step and every write happens after it.
 // HOIST selects the row loop: true reads the three input rows of each 3-row
 // trip before the trip's writes; false reads each row just before the row
 // above it is evaluated.  Both compute the same values; which is faster
@@ -638,9 +640,6 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
     }
     __syncthreads();
 
-    const int rows_per_warp = TH / WARPS;
-    const int rw0 = warp * rows_per_warp;
-    const int rw1 = rw0 + rows_per_warp;
 
     auto read_row = [&](int r, word (&C)[NB][V]) {
 #pragma unroll
@@ -725,8 +724,12 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
     };
 
     auto step = [&](int t, auto tp_tag) {
-        const int lo = max(rw0, t);
-        const int hi = min(rw1, TH - t);
+        // the valid rows t .. TH-1-t, split evenly over the warps (the region
+        // shrinks every step, so fixed bands would leave the edge warps idle)
+        const int total = TH - 2 * t;
+        const int base = total / WARPS, extra = total % WARPS;
+        const int lo = t + warp * base + min(warp, extra);
+        const int hi = lo + base + (warp < extra ? 1 : 0);
         word topC[NB][V], botC[NB][V];
         if (lo < hi) {
             read_row(lo - 1, topC);
