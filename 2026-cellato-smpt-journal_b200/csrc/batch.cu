@@ -154,7 +154,8 @@ int cellato_batch_create(int layout, int word_bits, const cellato_batch_grid* gr
         return cuda_fail(e, "cudaMemcpy (batch work lists)");
     }
 
-    // persistent CTAs: two per SM (the temporal tile is sized for two)
+    // persistent CTAs: as many per SM as the tile's shared memory and the
+    // kernel's registers allow
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -185,10 +186,11 @@ int cellato_batch_create(int layout, int word_bits, const cellato_batch_grid* gr
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
         b->streams.push_back(s);
         e = cudaStreamWaitEvent(s, fork, 0);
+        const int per_sm = ops_of(gp.rule)->batch_blocks_per_sm(b->internal, gp.TH);
         for (size_t r = 0; r < gp.rounds.size() && e == cudaSuccess; ++r) {
             const auto [first, count] = gp.rounds[r];
             if (count == 0) continue;
-            const int ctas = std::min(count, 2 * sms);
+            const int ctas = std::min(count, per_sm * sms);
             e = ops_of(gp.rule)->temporal_batch(b->internal, d_descs, d_items + first, count, (int)(r & 1),
                                                 (int)r * gp.k, gp.TH, gp.HY, ctas, s);
             ++b->launches;

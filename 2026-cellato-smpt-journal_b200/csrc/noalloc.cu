@@ -157,11 +157,12 @@ extern "C" int cellato_batch_run_noalloc(int layout, int word_bits, const cellat
         if (gp.rounds.empty()) continue;
         const rule_ops* ops = ops_of(gp.rule);
         if ((e = ops->prepare_batch(internal, gp.TH)) != cudaSuccess) return cuda_fail(e, "batch kernel attributes");
+        const int per_sm = ops->batch_blocks_per_sm(internal, gp.TH);
         for (size_t r = 0; r < gp.rounds.size(); ++r) {
             const auto [first, count] = gp.rounds[r];
             if (count == 0) continue;
             e = ops->temporal_batch(internal, d_descs, d_items + first, count, (int)(r & 1), (int)r * gp.k, gp.TH,
-                                    gp.HY, std::min(count, 2 * sms), s);
+                                    gp.HY, std::min(count, per_sm * sms), s);
             if (e != cudaSuccess) return cuda_fail(e, "batched temporal launch");
         }
     }

@@ -48,6 +48,8 @@ struct rule_ops {
     cudaError_t (*prepare_batch)(int layout, int TH);
     cudaError_t (*temporal_batch)(int layout, const batch_grid_desc* grids, const batch_item* items, int n_items,
                                   int parity, int t0, int TH, int HY, int ctas, cudaStream_t s);
+    // resident CTAs per SM of the batched kernel with a TH-row tile (after prepare_batch)
+    int (*batch_blocks_per_sm)(int layout, int TH);
     // state value of each dictionary index (index_to_state), 0 past `states`
     long long state_values[32];
 };
@@ -192,6 +194,25 @@ struct rule_kernels {
         return cudaErrorInvalidValue;
     }
 
+    static int batch_blocks_per_sm(int layout, int TH) {
+        int n = 0;
+        const size_t smem = tile_smem(TH);
+        const int threads = TEMPORAL_WARPS * 32;
+        cudaError_t e = cudaErrorInvalidValue;
+        switch (layout) {
+            case LAYOUT_LINEAR:
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<LAYOUT_LINEAR>(), threads, smem);
+                break;
+            case LAYOUT_TILED4:
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<LAYOUT_TILED4>(), threads, smem);
+                break;
+            case LAYOUT_TILED8:
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<LAYOUT_TILED8>(), threads, smem);
+                break;
+        }
+        return (e == cudaSuccess && n > 0) ? n : 1;
+    }
+
     static cudaError_t temporal_batch(int layout, const batch_grid_desc* grids, const batch_item* items, int n_items,
                                       int parity, int t0, int TH, int HY, int ctas, cudaStream_t s) {
         const size_t smem = tile_smem(TH);
@@ -214,7 +235,7 @@ struct rule_kernels {
 
     static rule_ops ops() {
         rule_ops o{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS,
-                   &take_wait_timeouts, &prepare_batch, &temporal_batch, {}};
+                   &take_wait_timeouts, &prepare_batch, &temporal_batch, &batch_blocks_per_sm, {}};
         static_assert(dict::number_of_values <= 32, "state table holds 32 values");
         for (int i = 0; i < dict::number_of_values; ++i)
             o.state_values[i] = static_cast<long long>(dict::index_to_state(i));

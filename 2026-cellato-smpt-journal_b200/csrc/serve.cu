@@ -80,6 +80,7 @@ struct cellato_server_st {
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[CELLATO_RULE_COUNT] = {};
     int TH[CELLATO_RULE_COUNT] = {}, HY[CELLATO_RULE_COUNT] = {};
+    int per_sm[CELLATO_RULE_COUNT] = {};  // resident CTAs per SM of each rule's batched kernel
     std::vector<slot> slots;
     int next_slot = 0;
     std::deque<inflight_rec> inflight;
@@ -286,6 +287,7 @@ int cellato_server_create(const cellato_server_config* cfg, cellato_server_t* ou
             destroy_all(s);
             return cuda_fail(e, "batch kernel attributes");
         }
+        s->per_sm[r] = ops->batch_blocks_per_sm(s->internal, s->TH[r]);
     }
     s->sched = sv::scheduler(lim);
 
@@ -434,7 +436,7 @@ int cellato_server_iterate(cellato_server_t s, int* active) {
                 return server_cuda_fail(s, e, "cudaStreamWaitEvent");
         }
         e = ops_of(L.rule)->temporal_batch(s->internal, d_descs, d_items + L.first, L.count, 0, 0, s->TH[L.rule],
-                                           s->HY[L.rule], std::min(L.count, 2 * s->sms), st);
+                                           s->HY[L.rule], std::min(L.count, s->per_sm[L.rule] * s->sms), st);
         if (e != cudaSuccess) return server_cuda_fail(s, e, "batched temporal launch (server)");
         ++s->launches;
     }
