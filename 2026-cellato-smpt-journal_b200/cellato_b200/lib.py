@@ -31,6 +31,7 @@ EXPORTED = [
     "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
     "cellato_batch_destroy", "cellato_batch_run_noalloc",
     "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random", "cellato_diff_cells",
+    "cellato_bit_array_bytes", "cellato_bit_array_to_planes", "cellato_planes_to_bit_array",
     "cellato_server_create", "cellato_server_submit_random", "cellato_server_submit_planes",
     "cellato_server_iterate", "cellato_server_poll", "cellato_server_planes", "cellato_server_release",
     "cellato_server_stats_get", "cellato_server_destroy", "cellato_server_submit_resume",
@@ -107,6 +108,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     ll = ctypes.c_longlong
     lib.cellato_checksum.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
     lib.cellato_diff_cells.argtypes = [i, _PP, _PP, ctypes.c_size_t, _vp, _vp]
+    lib.cellato_bit_array_bytes.argtypes = [i, i, i, i]
+    lib.cellato_bit_array_bytes.restype = ctypes.c_size_t
+    lib.cellato_bit_array_to_planes.argtypes = [i, i, _vp, i, i, i, i, _PP, _vp]
+    lib.cellato_planes_to_bit_array.argtypes = [i, i, i, _PP, i, i, i, _vp, _vp]
     lib.cellato_rule_state_value.argtypes = [i, i, ctypes.POINTER(ll)]
     lib.cellato_fill_random.argtypes = [i, i, i, _PP, i, i, ctypes.c_ulonglong, u32p, i, _vp]
     lib.cellato_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]
@@ -242,3 +247,16 @@ def diff_cells(nb: int, planes_a, planes_b, plane_bytes: int, count_ptr: int, st
     """Number of differing cells between two grids of the same layout, into one
     uint64 of device memory at count_ptr."""
     check(load().cellato_diff_cells(nb, ptr_array(planes_a), ptr_array(planes_b), plane_bytes, count_ptr, stream))
+
+
+def bit_array_to_planes(nb: int, array_word_bits: int, array_ptr: int, X: int, Y: int, layout: int, word_bits: int,
+                        planes, stream: int = 0) -> None:
+    """Device bit_array words -> device planes (the reference's bit_array layout)."""
+    check(load().cellato_bit_array_to_planes(nb, array_word_bits, array_ptr, X, Y, layout, word_bits,
+                                             ptr_array(planes), stream))
+
+
+def planes_to_bit_array(nb: int, layout: int, word_bits: int, planes, X: int, Y: int, array_word_bits: int,
+                        array_ptr: int, stream: int = 0) -> None:
+    check(load().cellato_planes_to_bit_array(nb, layout, word_bits, ptr_array(planes), X, Y, array_word_bits,
+                                             array_ptr, stream))

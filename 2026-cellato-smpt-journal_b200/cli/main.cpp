@@ -2,9 +2,11 @@
 //
 // Same flags, suite selection, CSV line (stdout) and report (stderr) as the
 // reference CLI (src/main.cpp:131-321, src/args-parser.hpp), restricted to the
-// CUDA bit-plane suites this library implements:
+// CUDA suites this library implements:
 //   --device CUDA --traverser simple|temporal --evaluator bit_planes|tiled_bit_planes
 //   --layout <same as evaluator> --word_size 32|64
+//   --device CUDA --traverser simple --evaluator bit_array --layout bit_array
+//   --word_size 32|64 (steps on bit planes; the grid converted on the device)
 // e.g.  cellato --automaton wire --device CUDA --traverser temporal \
 //         --evaluator tiled_bit_planes --layout tiled_bit_planes --word_size 64 \
 //         --x_size 16384 --y_size 16384 --steps 1000 --temporal_steps 8 --temporal_tile_size_y 0
@@ -116,7 +118,8 @@ int main(int argc, char** argv) {
         test::using_<std::uint32_t>::temporal_linear_bit_planes<A>,                                         \
         test::using_<std::uint64_t>::temporal_linear_bit_planes<A>,                                         \
         test::using_<std::uint32_t>::temporal_tiled_bit_planes<A>,                                          \
-        test::using_<std::uint64_t>::temporal_tiled_bit_planes<A>
+        test::using_<std::uint64_t>::temporal_tiled_bit_planes<A>,                                          \
+        test::using_<std::uint32_t>::bit_array<A>, test::using_<std::uint64_t>::bit_array<A>
     try {
         const bool ran =
             switch_<CELLATO_CASES(game_of_life::config), CELLATO_CASES(fire::config), CELLATO_CASES(wire::config),

@@ -247,6 +247,27 @@ int cellato_checksum(int rule, int layout, int word_bits, const void* const* pla
 int cellato_diff_cells(int nb, const void* const* planes_a, const void* const* planes_b, size_t plane_bytes,
                        unsigned long long* count, cellato_stream_t stream);
 
+/* ---- the bit_array layout --------------------------------------------------
+ * The reference's third layout (include/memory/bit_array_grid.hpp:80-322): a
+ * cell's nb index bits side by side, cells in row-major order, cpw =
+ * array_word_bits / nb cells per word, cell i in word i / cpw at bit
+ * (i % cpw) * nb; x_cells must be a multiple of cpw.  This library runs the
+ * steps on bit planes: a bit_array grid is converted on the device when a run
+ * starts and back when it ends (the C++ bit_array traverser does this), with
+ * the results of the reference's bit_array evaluator
+ * (include/evaluators/bit_array.hpp:73-105).  The planes' own layout and word
+ * size must be accepted by cellato_check_dims as well. */
+
+/* Bytes of the bit_array words of an X x Y grid, or 0 for bad arguments. */
+size_t cellato_bit_array_bytes(int nb, int array_word_bits, int x_cells, int y_cells);
+/* bit_array words (device) -> nb device planes in (layout, word_bits).
+ * Stream-ordered, no allocation. */
+int cellato_bit_array_to_planes(int nb, int array_word_bits, const void* array, int x_cells, int y_cells, int layout,
+                                int word_bits, void* const* planes, cellato_stream_t stream);
+/* nb device planes -> bit_array words (device).  Stream-ordered, no allocation. */
+int cellato_planes_to_bit_array(int nb, int layout, int word_bits, const void* const* planes, int x_cells,
+                                int y_cells, int array_word_bits, void* array, cellato_stream_t stream);
+
 /* State value of dictionary index `index` of a rule (index_to_state,
  * include/memory/state_dictionary.hpp:10-70). */
 int cellato_rule_state_value(int rule, int index, long long* value);

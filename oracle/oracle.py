@@ -85,6 +85,30 @@ class Oracle:
             raise ValueError("oracle_unpack rejected its arguments")
         return out
 
+    @staticmethod
+    def pack_bit_array(nb: int, word_bits: int, cells: np.ndarray) -> np.ndarray:
+        """The reference's bit_array layout (include/memory/bit_array_grid.hpp:
+        298-310 set_cell_at_index, :143-159): cells in row-major order,
+        cells_per_word = word_bits // nb, cell i in word i // cpw at bit
+        (i % cpw) * nb; the word count rounds up.  Returns the words."""
+        cpw = word_bits // nb
+        flat = np.ascontiguousarray(cells, dtype=np.uint8).reshape(-1).astype(np.uint64)
+        words = (flat.size + cpw - 1) // cpw
+        pad = np.zeros(words * cpw, dtype=np.uint64)
+        pad[:flat.size] = flat
+        shifts = np.arange(cpw, dtype=np.uint64) * np.uint64(nb)
+        w = np.bitwise_or.reduce(pad.reshape(words, cpw) << shifts, axis=1)
+        return w.astype(np.uint32 if word_bits == 32 else np.uint64)
+
+    @staticmethod
+    def unpack_bit_array(nb: int, word_bits: int, words: np.ndarray, X: int, Y: int) -> np.ndarray:
+        """Inverse of pack_bit_array (get_cell_at_index, bit_array_grid.hpp:312-320)."""
+        cpw = word_bits // nb
+        w = np.asarray(words).astype(np.uint64)
+        shifts = np.arange(cpw, dtype=np.uint64) * np.uint64(nb)
+        cells = (w[:, None] >> shifts) & np.uint64((1 << nb) - 1)
+        return cells.reshape(-1)[:X * Y].astype(np.uint8).reshape(Y, X)
+
     def checksum(self, rule: int, cells: np.ndarray) -> str:
         cells = np.ascontiguousarray(cells, dtype=np.uint8)
         Y, X = cells.shape
@@ -108,6 +132,8 @@ class RefOracle:
         lib.cref_pack.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p, ctypes.c_int,
                                   ctypes.c_int, _u8p]
         lib.cref_pack.restype = ctypes.c_longlong
+        lib.cref_pack_bit_array.argtypes = [ctypes.c_int, ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int, _u8p]
+        lib.cref_pack_bit_array.restype = ctypes.c_longlong
         lib.cref_reference_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p]
         lib.cref_checksum.argtypes = [ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                       ctypes.c_int]
@@ -155,6 +181,19 @@ class RefOracle:
         r = self.lib.cref_pack(rule, word_bits, int(tiled), _ptr(cells), X, Y, _ptr(out))
         if r < 0:
             raise RuntimeError("reference pack failed")
+        return out
+
+    def pack_bit_array(self, rule: int, word_bits: int, cells: np.ndarray) -> np.ndarray:
+        """Words of the reference's own bit_array grid built from `cells`."""
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        nb = self.planes(rule)
+        cpw = word_bits // nb
+        words = (X * Y + cpw - 1) // cpw
+        out = np.zeros(words, dtype=np.uint32 if word_bits == 32 else np.uint64)
+        r = self.lib.cref_pack_bit_array(rule, word_bits, _ptr(cells), X, Y, out.ctypes.data_as(_u8p))
+        if r < 0:
+            raise RuntimeError("reference bit_array pack failed")
         return out
 
     def reference_init(self, rule: int, X: int, Y: int, seed: int) -> np.ndarray:

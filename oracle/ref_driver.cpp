@@ -13,8 +13,9 @@
 //   * CPU bit_planes / tiled_bit_planes paths (same traverser, the
 //     bit-plane evaluators include/evaluators/bit_planes.hpp:45-663 and
 //     include/evaluators/tiled_bit_planes.hpp:60-396) -- a secondary check.
-//   * grid packing of include/memory/bit_planes_grid.hpp:234-270 and
-//     include/memory/tiled_bit_planes_grid.hpp:243-288, used to pin layouts.
+//   * grid packing of include/memory/bit_planes_grid.hpp:234-270,
+//     include/memory/tiled_bit_planes_grid.hpp:243-288 and
+//     include/memory/bit_array_grid.hpp:143-159, 298-310, used to pin layouts.
 //   * the reference's seeded initialisers src/<automaton>/data_init.hpp.
 //   * the 4x4 tile-sum checksum include/memory/standard_grid.hpp:179-213.
 //
@@ -37,6 +38,7 @@
 #include "memory/standard_grid.hpp"
 #include "memory/bit_planes_grid.hpp"
 #include "memory/tiled_bit_planes_grid.hpp"
+#include "memory/bit_array_grid.hpp"
 #include "traversers/cpu/simple.hpp"
 #include "traversers/traverser_utils.hpp"
 
@@ -189,6 +191,20 @@ long long pack(const uint8_t* in, int X, int Y, uint8_t* planes_out) {
     return (long long)(words * sizeof(W));
 }
 
+// Pack through the reference bit_array grid; words_out receives its words.
+template <typename A, typename W>
+long long pack_bit_array(const uint8_t* in, int X, int Y, uint8_t* words_out) {
+    using cell_t = cell_of<A>;
+    using grid_t = grids::bit_array::grid<typename A::state_dictionary, W>;
+    const std::size_t n = std::size_t(X) * Y;
+    auto st = to_states<A>(in, n);
+    grids::standard::grid<cell_t> sg(std::move(st), X, Y);
+    grid_t g(sg);
+    const std::size_t words = (n + grid_t::cells_per_word - 1) / grid_t::cells_per_word;
+    std::memcpy(words_out, g.raw_data(), words * sizeof(W));
+    return (long long)(words * sizeof(W));
+}
+
 template <typename A>
 int reference_init(int X, int Y, int seed, uint8_t* out) {
     cellato::run::run_params params;
@@ -300,6 +316,20 @@ long long cref_pack(int rule, int word_bits, int tiled, const uint8_t* in, int X
             if (word_bits == 64 && !tiled) r = pack<A, uint64_t, false>(in, X, Y, planes_out);
             if (word_bits == 32 && tiled) r = pack<A, uint32_t, true>(in, X, Y, planes_out);
             if (word_bits == 64 && tiled) r = pack<A, uint64_t, true>(in, X, Y, planes_out);
+            return 0;
+        });
+        return r;
+    } catch (...) {
+        return -2;
+    }
+}
+
+long long cref_pack_bit_array(int rule, int word_bits, const uint8_t* in, int X, int Y, uint8_t* words_out) {
+    try {
+        long long r = -1;
+        with_rule(rule, [&]<typename A>() {
+            if (word_bits == 32) r = pack_bit_array<A, uint32_t>(in, X, Y, words_out);
+            if (word_bits == 64) r = pack_bit_array<A, uint64_t>(in, X, Y, words_out);
             return 0;
         });
         return r;

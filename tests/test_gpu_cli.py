@@ -52,3 +52,26 @@ def test_cli_rejects_unknown_suite_and_reports_bad_sizes(cuda):
                         "--evaluator", "bit_planes", "--layout", "bit_planes", "--word_size", "64",
                         "--x_size", "96", "--y_size", "8", "--steps", "1"], capture_output=True, text=True)
     assert r.returncode == 3
+
+
+@pytest.mark.parametrize("word,X", [(32, 480), (64, 1344)])
+def test_cli_bit_array_checksums_match_reference(cuda, word, X):
+    """The reference's bit_array suite (--evaluator bit_array --layout bit_array,
+    the simple traverser): a bit_array grid built from the reference's seeded
+    state, converted to planes on the device, stepped, converted back.  The widths
+    are multiples of 32 and of every rule's cells per word."""
+    from oracle import RefOracle
+    ref = RefOracle()
+    header = run_cli(["--print_csv_header"]).split(",")
+    Y, steps, seed = 40, 17, 11
+    for rule, name in enumerate(RULES):
+        if name == "wire":
+            continue
+        args = ["--automaton", name, "--device", "CUDA", "--traverser", "simple", "--evaluator", "bit_array",
+                "--layout", "bit_array", "--word_size", str(word), "--x_size", str(X), "--y_size", str(Y),
+                "--steps", str(steps), "--seed", str(seed), "--rounds", "2"]
+        row = dict(zip(header, run_cli(args).split(",")))
+        cells = ref.reference_init(rule, X, Y, seed)
+        want = ref.checksum(rule, ref.run_standard(rule, cells, steps))
+        assert row["checksum"] == want, (name, word)
+        assert row["rounds_had_same_checksums"] == "true"

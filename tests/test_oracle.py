@@ -62,3 +62,24 @@ def test_layout_known_answers(oracle):
     # tiled 8x4: cell (33, 1) -> tile (4, 0), bit 1*8 + 1
     t32 = oracle.pack(1, 32, 1, cells)[0].view(np.uint32)
     assert t32[4] == (1 << 9)
+
+
+def test_bit_array_layout_matches_reference(oracle):
+    """The oracle's restatement of the bit_array layout against the words of the
+    reference's own bit_array grid, for every rule and both word sizes."""
+    from oracle import RefOracle
+    try:
+        ref = RefOracle()
+    except FileNotFoundError:
+        pytest.skip("reference CPU library not built")
+    rng = np.random.default_rng(17)
+    for r in range(10):
+        nb = oracle.planes(r)
+        for W in (32, 64):
+            cpw = W // nb
+            X, Y = cpw * 7, 13
+            cells = rng.integers(0, oracle.states(r), size=(Y, X), dtype=np.uint8)
+            want = ref.pack_bit_array(r, W, cells)
+            got = oracle.pack_bit_array(nb, W, cells)
+            assert got.dtype == want.dtype and np.array_equal(got, want), (RULES[r], W)
+            assert np.array_equal(oracle.unpack_bit_array(nb, W, got, X, Y), cells)
