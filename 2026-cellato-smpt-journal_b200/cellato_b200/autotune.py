@@ -24,8 +24,12 @@ from . import lib
 # many planes or long networks reaches more of the HBM roofline.
 SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1)) + tuple(
     ("temporal", 1, th, loop) for th in (0, 96, 128) for loop in (1, 2))
+# (mode, k, tile_rows, row loop, words per lane); words per lane as
+# cellato_set_temporal_width (0 = the rule's default; 1 differs from it only for
+# rules of up to three planes, and is skipped for the others)
 DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2),) + tuple(
-    ("temporal", k, th, loop) for k in (4, 6, 8, 12, 16) for th in (0, 96, 128, 160, 192) for loop in (1, 2))
+    ("temporal", k, th, loop, width) for k in (4, 6, 8, 12, 16) for th in (0, 96, 128, 160, 192)
+    for loop in (1, 2) for width in (0, 1))
 _VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2}
 
 _lock = threading.Lock()
@@ -43,7 +47,7 @@ def cache_path() -> str:
 
 
 def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
-    return f"v4/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+    return f"v5/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
 
 
 def _load_file() -> dict:
@@ -77,11 +81,13 @@ def run(choice: dict, rule: int, layout: int, word_bits: int, planes_a, planes_b
         finally:
             lib.set_simple_variant(0)
     lib.set_temporal_variant(choice.get("loop", 0))
+    lib.set_temporal_width(choice.get("width", 0))
     try:
         return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
                                 choice.get("tile_rows", 0), stream)
     finally:
         lib.set_temporal_variant(0)
+        lib.set_temporal_width(0)
 
 
 def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, candidates=DEFAULT_CANDIDATES,
@@ -111,9 +117,12 @@ def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, 
         mode, k = cand[0], cand[1]
         th = cand[2] if len(cand) > 2 else 0
         loop = cand[3] if len(cand) > 3 else 0
+        width = cand[4] if len(cand) > 4 else 0
         if th and th - 2 * ((k + 7) // 8 * 8) < 8:
             continue  # the halos would leave no interior
-        choice = {"mode": mode, "k": k, "tile_rows": th, "loop": loop}
+        if width == 1 and lib.rule_planes(rule) > 3:
+            continue  # one word per lane is already these rules' default
+        choice = {"mode": mode, "k": k, "tile_rows": th, "loop": loop, "width": width}
         steps = max(burst_steps, 2 * k) // k * k
         try:
             run(choice, rule, layout, word_bits, planes_a, planes_b, X, Y, 0, k, stream)  # warm-up

@@ -28,6 +28,7 @@ EXPORTED = [
     "cellato_pack_cells", "cellato_unpack_cells",
     "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
     "cellato_device_wait_timeouts", "cellato_set_simple_variant", "cellato_set_temporal_variant",
+    "cellato_set_temporal_width",
     "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
     "cellato_batch_destroy", "cellato_batch_run_noalloc",
     "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random", "cellato_diff_cells",
@@ -191,6 +192,11 @@ def set_simple_variant(variant: int) -> None:
 def set_temporal_variant(variant: int) -> None:
     """0 automatic, 1 row-by-row reads, 2 hoisted reads per three-row trip (temporal kernel)."""
     check(load().cellato_set_temporal_variant(variant))
+
+
+def set_temporal_width(words_per_lane: int) -> None:
+    """0 the rule's default, 1 or 2 words per lane of the temporal kernel."""
+    check(load().cellato_set_temporal_width(words_per_lane))
 
 
 def device_wait_timeouts() -> int:

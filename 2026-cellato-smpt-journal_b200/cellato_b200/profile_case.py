@@ -28,12 +28,14 @@ def main() -> None:
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--loop", type=int, default=0, help="temporal row loop (cellato_set_temporal_variant)")
+    ap.add_argument("--width", type=int, default=0, help="temporal words per lane (cellato_set_temporal_width)")
     ap.add_argument("--launches", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     a = ap.parse_args()
 
     r = lib.rule_id(a.rule)
     lib.set_temporal_variant(a.loop)
+    lib.set_temporal_width(a.width)
     nb = lib.rule_planes(r)
     layout = lib.LAYOUTS[a.layout]
     X = Y = a.size

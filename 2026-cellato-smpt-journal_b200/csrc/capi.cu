@@ -95,8 +95,8 @@ int max_optin_smem() {
 // Taller tiles waste less on halos but leave fewer CTAs for the 148 SMs and
 // fewer resident warps per SM; measured on B200 at 16384^2 over the ten rules,
 // this height is within a few percent of the best single height per rule.
-int default_tile_rows(const rule_ops* ops, int R, int k) {
-    const int row_bytes = ops->planes * 32 * ops->temporal_words_per_lane * 4;
+int default_tile_rows(const rule_ops* ops, int R, int k, int V) {
+    const int row_bytes = ops->planes * 32 * V * 4;
     const int q = std::max(ops->temporal_warps, R);
     const int HY = (std::max(1, k) + R - 1) / R * R;
     const int two_per_sm = (113 * 1024) / row_bytes / q * q;
@@ -227,6 +227,13 @@ int cellato_set_simple_variant(int variant) {
     return CELLATO_OK;
 }
 
+int cellato_set_temporal_width(int words_per_lane) {
+    if (words_per_lane < 0 || words_per_lane > 2)
+        return fail(CELLATO_EINVAL, "temporal words per lane must be 0, 1 or 2");
+    temporal_width() = words_per_lane;
+    return CELLATO_OK;
+}
+
 int cellato_set_temporal_variant(int variant) {
     if (variant < 0 || variant > 2) return fail(CELLATO_EINVAL, "temporal kernel variant must be 0, 1 or 2");
     temporal_variant() = variant;
@@ -268,10 +275,11 @@ int cellato_run_temporal(int rule, int layout, int word_bits, void* const* plane
     const int L = internal_layout(layout, word_bits);
     const int R = band_height(layout, word_bits);
     const int q = std::max(ops->temporal_warps, R);
-    const int TH = tile_rows > 0 ? tile_rows : default_tile_rows(ops, R, k);
+    const int V = ops->temporal_v_now();
+    const int TH = tile_rows > 0 ? tile_rows : default_tile_rows(ops, R, k, V);
     if (TH % q != 0)
         return fail(CELLATO_EINVAL, "temporal tile rows %d must be a multiple of %d", TH, q);
-    const int row_bytes = ops->planes * 32 * ops->temporal_words_per_lane * 4;
+    const int row_bytes = ops->planes * 32 * V * 4;
     if ((long long)TH * row_bytes > max_optin_smem())
         return fail(CELLATO_ESMEM, "Configuration exceeds maximum shared memory size. The temporal tile is too large.");
     const int Xw = x_cells / 32;

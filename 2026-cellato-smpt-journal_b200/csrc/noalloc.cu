@@ -95,7 +95,7 @@ extern "C" int cellato_batch_run_noalloc(int layout, int word_bits, const cellat
         const int k = k_per_rule ? k_per_rule[r] : 0;
         groups[r].rule = r;
         groups[r].k = k > 0 ? std::min(k, 32) : 8;
-        groups[r].TH = default_tile_rows(ops_of(r), R, groups[r].k);
+        groups[r].TH = default_tile_rows(ops_of(r), R, groups[r].k, ops_of(r)->temporal_words_per_lane);
         groups[r].HY = (groups[r].k + R - 1) / R * R;
     }
     for (int i = 0; i < n_grids; ++i) {

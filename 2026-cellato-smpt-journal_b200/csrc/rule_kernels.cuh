@@ -29,6 +29,15 @@ inline int& temporal_variant() {
     return v;
 }
 
+// Words per lane of the single-grid temporal kernel: 0 = the rule's default
+// (two for rules of up to three planes, else one), 1 = one word per lane (half
+// the registers and shared memory per row, so more CTAs per SM), 2 = two (rules
+// of up to three planes only; others use one).  Process-wide.
+inline int& temporal_width() {
+    static int v = 0;
+    return v;
+}
+
 struct rule_ops {
     const char* name;
     int planes;  // needed_bits
@@ -39,7 +48,8 @@ struct rule_ops {
     // k fused steps from t0 on a TH-row tile with an HY-row halo
     cudaError_t (*temporal)(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                             int TH, int HY, cudaStream_t s);
-    int temporal_words_per_lane;  // V of the temporal tile (tile width 32*V words)
+    int temporal_words_per_lane;  // default V of the temporal tile (tile width 32*V words); the batched kernel's V
+    int (*temporal_v_now)();      // V that `temporal` uses under the current cellato_set_temporal_width
     int temporal_warps;
     // reads and clears the count of bounded waits that gave up (device-side)
     cudaError_t (*take_wait_timeouts)(unsigned* count);
@@ -150,10 +160,20 @@ struct rule_kernels {
         return cudaErrorInvalidValue;
     }
 
+    static int temporal_v_now() { return (TEMPORAL_V == 2 && temporal_width() != 1) ? 2 : 1; }
+
     template <int LAYOUT>
     static cudaError_t temporal_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                                        int TH, int HY, cudaStream_t s) {
-        constexpr int V = TEMPORAL_V;
+        if constexpr (TEMPORAL_V == 2) {
+            if (temporal_width() != 1) return temporal_launch<LAYOUT, 2>(in, out, Xw, Y, t0, k, TH, HY, s);
+        }
+        return temporal_launch<LAYOUT, 1>(in, out, Xw, Y, t0, k, TH, HY, s);
+    }
+
+    template <int LAYOUT, int V>
+    static cudaError_t temporal_launch(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
+                                       int TH, int HY, cudaStream_t s) {
         auto kern = temporal_variant() == 1 ? temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, false>
                                             : temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, true>;
         const size_t smem = (size_t)NB * TH * 32 * V * sizeof(word);
@@ -234,7 +254,7 @@ struct rule_kernels {
     }
 
     static rule_ops ops() {
-        rule_ops o{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, TEMPORAL_WARPS,
+        rule_ops o{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, &temporal_v_now, TEMPORAL_WARPS,
                    &take_wait_timeouts, &prepare_batch, &temporal_batch, &batch_blocks_per_sm, {}};
         static_assert(dict::number_of_values <= 32, "state table holds 32 values");
         for (int i = 0; i < dict::number_of_values; ++i)

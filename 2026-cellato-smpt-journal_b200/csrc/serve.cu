@@ -277,7 +277,7 @@ int cellato_server_create(const cellato_server_config* cfg, cellato_server_t* ou
     lim.chunk_rounds = cfg->chunk_rounds > 0 ? cfg->chunk_rounds : 4;
     for (int r = 0; r < CELLATO_RULE_COUNT; ++r) {
         const rule_ops* ops = ops_of(r);
-        s->TH[r] = default_tile_rows(ops, s->R, lim.k[r]);
+        s->TH[r] = default_tile_rows(ops, s->R, lim.k[r], ops->temporal_words_per_lane);
         s->HY[r] = (lim.k[r] + s->R - 1) / s->R * s->R;
         if (s->TH[r] - 2 * s->HY[r] <= 0) {
             destroy_all(s);

@@ -64,7 +64,8 @@ def parse():
     ap.add_argument("--ca-steps", type=int, default=None, help="steps per automaton (default: the workload's)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--choice", default="", help="pin the traverser per automaton instead of autotuning, "
-                                                 "e.g. wire=temporal:8:128:1,excitable=temporal:16:0:2")
+                                                 "e.g. wire=temporal:8:128:1,excitable=temporal:16:0:2:1 "
+                                                 "(mode:k:tile_rows:loop:words_per_lane)")
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "batched", "served"],
                     help="config2: WireWorld + Greenberg-Hastings 16384^2 x 1000 steps (default); "
                          "config3: cyclic + HPP fluid 32768^2 x 256 steps on bit_planes, with the single-step "
@@ -249,7 +250,7 @@ def reference_arm(args, rank: int, world: int):
 
 
 def parse_choices(text: str) -> dict:
-    """--choice wire=temporal:8:128:1,excitable=temporal:16:0:2 (mode:k:tile_rows:loop)
+    """--choice wire=temporal:8:128:1,excitable=temporal:16:0:2:1 (mode:k:tile_rows:loop:words_per_lane)
     or <automaton>=simple_register / simple_stream: pins the traverser per automaton."""
     out = {}
     for item in filter(None, (text or "").split(",")):
@@ -257,7 +258,7 @@ def parse_choices(text: str) -> dict:
         f = spec.split(":")
         if f[0] == "temporal":
             out[name] = {"mode": "temporal", "k": int(f[1]), "tile_rows": int(f[2]) if len(f) > 2 else 0,
-                         "loop": int(f[3]) if len(f) > 3 else 0}
+                         "loop": int(f[3]) if len(f) > 3 else 0, "width": int(f[4]) if len(f) > 4 else 0}
         else:
             out[name] = {"mode": f[0], "k": 1, "tile_rows": 0}
     return out
@@ -268,7 +269,8 @@ def describe_choice(c: dict) -> str:
     if c["mode"] != "temporal":
         return c["mode"]
     loop = {0: "default", 1: "row-by-row", 2: "hoisted"}[c.get("loop", 0)]
-    return f"temporal k={c['k']} tile_rows={c.get('tile_rows', 0)} loop={loop}"
+    width = {0: "default", 1: "1", 2: "2"}[c.get("width", 0)]
+    return f"temporal k={c['k']} tile_rows={c.get('tile_rows', 0)} loop={loop} words_per_lane={width}"
 
 
 def workload_config(args, extra=None):

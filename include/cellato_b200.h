@@ -159,6 +159,16 @@ int cellato_set_simple_variant(int variant);
  * reference (one temporal kernel). */
 int cellato_set_temporal_variant(int variant);
 
+/* Words per lane of the temporal kernel (cellato_run_temporal): 0 = the rule's
+ * default (2 for rules of up to three planes, else 1), 1 = one word per lane
+ * (half the registers and shared memory per tile row, so more CTAs per SM),
+ * 2 = two (rules of up to three planes; others use one).  Same results; the
+ * tile is 32 x words-per-lane words wide, so default tile heights and
+ * cellato_temporal_max_tile_rows follow the setting.  Process-wide, not
+ * synchronised with concurrent launches; the autotuner sweeps it.  No
+ * counterpart in the reference. */
+int cellato_set_temporal_width(int words_per_lane);
+
 /* Reads and clears the number of bounded device-side waits (mbarrier waits of
  * the streaming single-step kernel) that gave up since the last call; returns
  * CELLATO_ETIMEDOUT when it is non-zero.  Synchronises the device.  No

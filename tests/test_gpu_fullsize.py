@@ -60,14 +60,19 @@ def checksum(rule, layout, p, X, Y):
     return sums.cpu().tolist()
 
 
-@pytest.mark.parametrize("rule,k,th,loop", [("wire", 8, 128, 1), ("wire", 16, 0, 2),
-                                            ("excitable", 16, 0, 2), ("excitable", 8, 128, 1)])
-def test_config2_size_temporal_equals_single_step(cuda, rule, k, th, loop):
+@pytest.mark.parametrize("rule,k,th,loop,width", [("wire", 8, 128, 1, 0), ("wire", 16, 0, 2, 0),
+                                                  ("excitable", 16, 0, 2, 0), ("excitable", 8, 128, 1, 0),
+                                                  ("excitable", 16, 192, 2, 1), ("wire", 16, 192, 1, 1)])
+def test_config2_size_temporal_equals_single_step(cuda, rule, k, th, loop, width):
     import torch
     r = lib.rule_id(rule)
     S, steps = 16384, 48
     ref = run(r, 1, S, S, steps, 42, "simple")
-    got = run(r, 1, S, S, steps, 42, "temporal", k, th, loop)
+    lib.set_temporal_width(width)
+    try:
+        got = run(r, 1, S, S, steps, 42, "temporal", k, th, loop)
+    finally:
+        lib.set_temporal_width(0)
     assert diff(inputs.PLANES[r], ref, got) == 0
     assert checksum(r, 1, ref, S, S) == checksum(r, 1, got, S, S)
     del ref, got

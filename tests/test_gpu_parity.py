@@ -49,19 +49,23 @@ def test_temporal_small_golden(cuda, oracle, golden_small, layout, W, k):
         assert np.array_equal(out, cout), (case["key"], case["rule"], k, int((out != cout).sum()))
 
 
+@pytest.mark.parametrize("width", [0, 1])
 @pytest.mark.parametrize("loop", [1, 2])
 @pytest.mark.parametrize("k", [3, 8])
 @pytest.mark.parametrize("layout,W", LAYOUTS)
-def test_temporal_row_loops(cuda, oracle, golden_small, layout, W, k, loop):
-    """Both row loops of the temporal kernel (cellato_set_temporal_variant)."""
+def test_temporal_row_loops(cuda, oracle, golden_small, layout, W, k, loop, width):
+    """Both row loops (cellato_set_temporal_variant) and both tile widths
+    (cellato_set_temporal_width) of the temporal kernel."""
     lib.set_temporal_variant(loop)
+    lib.set_temporal_width(width)
     try:
         for case, cin, cout in golden_small:
             r = RULES.index(case["rule"])
             out = run_gpu(oracle, r, layout, W, cin, case["steps"], mode="temporal", k=k, tile_rows=48)
-            assert np.array_equal(out, cout), (case["key"], case["rule"], k, loop)
+            assert np.array_equal(out, cout), (case["key"], case["rule"], k, loop, width)
     finally:
         lib.set_temporal_variant(0)
+        lib.set_temporal_width(0)
 
 
 @pytest.mark.parametrize("mode,k", [("simple", 1), ("temporal", 3), ("temporal", 8)])
