@@ -28,7 +28,7 @@ SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1)) + tuple(
 # cellato_set_temporal_width (0 = the rule's default; 1 differs from it only for
 # rules of up to three planes, and is skipped for the others)
 DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2),) + tuple(
-    ("temporal", k, th, loop, width) for k in (4, 6, 8, 12, 16) for th in (0, 96, 128, 160, 192)
+    ("temporal", k, th, loop, width) for k in (4, 6, 8, 12, 16, 24) for th in (0, 96, 128, 160, 192, 256, 320)
     for loop in (1, 2) for width in (0, 1))
 _VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2}
 
@@ -47,7 +47,7 @@ def cache_path() -> str:
 
 
 def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
-    return f"v5/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+    return f"v6/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
 
 
 def _load_file() -> dict:

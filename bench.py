@@ -89,19 +89,21 @@ def parse():
     return args
 
 
-# workload -> (automata, side, steps per automaton, layout)
+# workload -> (automata, side, steps per automaton, layout, largest k the
+# workload's definition lets the autotuner pick)
 SINGLE_GRID_WORKLOADS = {
-    "config2": (("wire", "excitable"), SIZE, CA_STEPS, 1),
-    "config3": (("cyclic", "fluid"), 32768, 256, 0),
+    "config2": (("wire", "excitable"), SIZE, CA_STEPS, 1, 16),   # "temporal depth k autotuned in 1-16"
+    "config3": (("cyclic", "fluid"), 32768, 256, 0, 32),
 }
+K_MAX = 16
 
 
 def apply_workload(args) -> None:
     """Sets the automata, sizes and layout of a single-grid workload."""
-    global AUTOMATA, LAYOUT
-    automata, side, steps, layout = SINGLE_GRID_WORKLOADS.get(args.workload, SINGLE_GRID_WORKLOADS["config2"])
+    global AUTOMATA, LAYOUT, K_MAX
+    automata, side, steps, layout, kmax = SINGLE_GRID_WORKLOADS.get(args.workload, SINGLE_GRID_WORKLOADS["config2"])
     if args.workload in SINGLE_GRID_WORKLOADS:
-        AUTOMATA, LAYOUT = automata, layout
+        AUTOMATA, LAYOUT, K_MAX = automata, layout, kmax
     args.size = args.size or side
     args.ca_steps = args.ca_steps or steps
 
@@ -278,7 +280,7 @@ def workload_config(args, extra=None):
     layout = "tiled_bit_planes" if LAYOUT == 1 else "bit_planes"
     mib = [2 * inputs.PLANES[inputs.RULE_ID[a]] * args.size * args.size // 8 >> 20 for a in AUTOMATA]
     c = {"workload": f"{'+'.join(AUTOMATA)} {args.size}x{args.size} {layout} W{WORD_BITS}, {args.ca_steps} steps "
-                     f"each, traverser autotuned (simple | temporal k)",
+                     f"each, traverser autotuned (simple | temporal k <= {K_MAX})",
          "automata": list(AUTOMATA), "x_size": args.size, "y_size": args.size, "ca_steps_per_step": args.ca_steps,
          "layout": layout, "word_size": WORD_BITS,
          "l2": f"inputs larger than L2 (ping-pong planes {' MiB + '.join(str(m) for m in mib)} MiB), no flush"}
@@ -315,8 +317,9 @@ def our_arm(args, rank: int, world: int):
     # autotune per automaton (on scratch copies of the planes), unless pinned
     pinned = parse_choices(args.choice)
     for a, g in grids.items():
+        cands = [c for c in autotune.DEFAULT_CANDIDATES if c[1] <= K_MAX]
         choice = pinned.get(a) or autotune.tune(g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y,
-                                                use_cache=False)
+                                                candidates=cands, use_cache=False)
         g["choice"] = choice
         g["a"].buf.copy_(g["init"].buf)
     torch.cuda.synchronize()
