@@ -78,7 +78,7 @@ int cellato_batch_create(int layout, int word_bits, const cellato_batch_grid* gr
         groups[r].rule = r;
         const int k = k_per_rule ? k_per_rule[r] : 0;
         groups[r].k = k > 0 ? std::min(k, 32) : 8;
-        groups[r].TH = default_tile_rows(ops_of(r), b->R, groups[r].k, ops_of(r)->temporal_words_per_lane);
+        groups[r].TH = default_tile_rows(ops_of(r), b->R, groups[r].k, ops_of(r)->batch_words_per_lane);
         groups[r].HY = (groups[r].k + b->R - 1) / b->R * b->R;
     }
     for (int i = 0; i < n_grids; ++i) {
@@ -114,7 +114,7 @@ int cellato_batch_create(int layout, int word_bits, const cellato_batch_grid* gr
     for (auto& gp : groups) {
         if (gp.grids.empty()) continue;
         const rule_ops* ops = ops_of(gp.rule);
-        const int TW = 32 * ops->temporal_words_per_lane;
+        const int TW = 32 * ops->batch_words_per_lane;
         const int effW = TW - 2, effH = gp.TH - 2 * gp.HY;
         if (effH <= 0) {
             release(b);

@@ -257,7 +257,7 @@ int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits) {
     if (!ops) return -fail(CELLATO_EINVAL, "unknown rule id %d", rule);
     if (word_bits != 32 && word_bits != 64) return -fail(CELLATO_EINVAL, "word_bits must be 32 or 64");
     const int R = band_height(layout, word_bits);
-    const int row_bytes = ops->planes * 32 * ops->temporal_words_per_lane * 4;
+    const int row_bytes = ops->planes * 32 * ops->temporal_v_now() * 4;
     const int q = std::max(ops->temporal_warps, R);
     return (max_optin_smem() / row_bytes) / q * q;
 }

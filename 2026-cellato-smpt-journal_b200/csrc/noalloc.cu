@@ -95,7 +95,7 @@ extern "C" int cellato_batch_run_noalloc(int layout, int word_bits, const cellat
         const int k = k_per_rule ? k_per_rule[r] : 0;
         groups[r].rule = r;
         groups[r].k = k > 0 ? std::min(k, 32) : 8;
-        groups[r].TH = default_tile_rows(ops_of(r), R, groups[r].k, ops_of(r)->temporal_words_per_lane);
+        groups[r].TH = default_tile_rows(ops_of(r), R, groups[r].k, ops_of(r)->batch_words_per_lane);
         groups[r].HY = (groups[r].k + R - 1) / R * R;
     }
     for (int i = 0; i < n_grids; ++i) {
@@ -117,7 +117,7 @@ extern "C" int cellato_batch_run_noalloc(int layout, int word_bits, const cellat
     std::vector<batch_item> items;
     for (auto& gp : groups) {
         if (gp.grids.empty()) continue;
-        const int effW = 32 * ops_of(gp.rule)->temporal_words_per_lane - 2, effH = gp.TH - 2 * gp.HY;
+        const int effW = 32 * ops_of(gp.rule)->batch_words_per_lane - 2, effH = gp.TH - 2 * gp.HY;
         if (effH <= 0) return fail(CELLATO_EINVAL, "rule %d: tile leaves no interior for k=%d", gp.rule, gp.k);
         int max_rounds = 0;
         for (int i : gp.grids) max_rounds = std::max(max_rounds, rounds[i]);

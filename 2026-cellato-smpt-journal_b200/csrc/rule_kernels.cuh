@@ -48,8 +48,9 @@ struct rule_ops {
     // k fused steps from t0 on a TH-row tile with an HY-row halo
     cudaError_t (*temporal)(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                             int TH, int HY, cudaStream_t s);
-    int temporal_words_per_lane;  // default V of the temporal tile (tile width 32*V words); the batched kernel's V
+    int temporal_words_per_lane;  // default V of the temporal tile (tile width 32*V words)
     int (*temporal_v_now)();      // V that `temporal` uses under the current cellato_set_temporal_width
+    int batch_words_per_lane;     // V of the batched temporal kernel
     int temporal_warps;
     // reads and clears the count of bounded waits that gave up (device-side)
     cudaError_t (*take_wait_timeouts)(unsigned* count);
@@ -83,6 +84,10 @@ struct rule_kernels {
     static_assert(NB <= MAX_PLANES, "too many planes");
     static constexpr int SIMPLE_WARPS = 4;
     static constexpr int TEMPORAL_V = NB <= 3 ? 2 : 1;
+    // The batched kernel runs one word per lane: its tiles are 32 words wide,
+    // which wastes less on the narrow grids of a batch, and its register use
+    // leaves room for three CTAs per SM.
+    static constexpr int BATCH_V = 1;
     static constexpr int TEMPORAL_WARPS = 8;
 
     template <int LAYOUT, int V>
@@ -197,9 +202,9 @@ struct rule_kernels {
 
     template <int LAYOUT>
     static auto batch_kernel() {
-        return temporal_batch_kernel<net, NB, LAYOUT, TEMPORAL_V, TEMPORAL_WARPS>;
+        return temporal_batch_kernel<net, NB, LAYOUT, BATCH_V, TEMPORAL_WARPS>;
     }
-    static size_t tile_smem(int TH) { return (size_t)NB * TH * 32 * TEMPORAL_V * sizeof(word); }
+    static size_t tile_smem(int TH) { return (size_t)NB * TH * 32 * BATCH_V * sizeof(word); }
 
     static cudaError_t prepare_batch(int layout, int TH) {
         const int smem = (int)tile_smem(TH);
@@ -254,7 +259,8 @@ struct rule_kernels {
     }
 
     static rule_ops ops() {
-        rule_ops o{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, &temporal_v_now, TEMPORAL_WARPS,
+        rule_ops o{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, &temporal_v_now, BATCH_V,
+                   TEMPORAL_WARPS,
                    &take_wait_timeouts, &prepare_batch, &temporal_batch, &batch_blocks_per_sm, {}};
         static_assert(dict::number_of_values <= 32, "state table holds 32 values");
         for (int i = 0; i < dict::number_of_values; ++i)

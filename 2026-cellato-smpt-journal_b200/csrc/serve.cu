@@ -236,7 +236,7 @@ int submit_common(cellato_server_t s, int rule, int x, int y, int steps, int t0,
     r.t0 = t0;
     r.plane_bytes = (size_t)x * y / 8;
     r.stride = round_up(r.plane_bytes, ALIGN);
-    const int effW = 32 * ops->temporal_words_per_lane - 2, effH = s->TH[rule] - 2 * s->HY[rule];
+    const int effW = 32 * ops->batch_words_per_lane - 2, effH = s->TH[rule] - 2 * s->HY[rule];
     const int tiles = ((x / 32 + effW - 1) / effW) * ((y + effH - 1) / effH);
     r.submit_s = s->now();
     *id = s->sched.submit(rule, x, y, steps, (long long)(2 * (size_t)r.nb * r.stride), tiles, r.keep, t0 & 1);
@@ -273,11 +273,13 @@ int cellato_server_create(const cellato_server_config* cfg, cellato_server_t* ou
         return cuda_fail(e, "querying the device");
     }
     lim.cap_bytes = cfg->hbm_cap_bytes ? (long long)cfg->hbm_cap_bytes : (long long)(0.8 * (double)total_b);
-    lim.tile_budget = cfg->tile_budget > 0 ? cfg->tile_budget : 16LL * s->sms;
+    // default budget: 1024 tile words per SM per round (32 one-word-per-lane tiles), about seven waves of
+    // three CTAs per SM, enough to fill the device with each automaton's launch
+    lim.tile_budget = cfg->tile_budget > 0 ? cfg->tile_budget : 32LL * s->sms;
     lim.chunk_rounds = cfg->chunk_rounds > 0 ? cfg->chunk_rounds : 4;
     for (int r = 0; r < CELLATO_RULE_COUNT; ++r) {
         const rule_ops* ops = ops_of(r);
-        s->TH[r] = default_tile_rows(ops, s->R, lim.k[r], ops->temporal_words_per_lane);
+        s->TH[r] = default_tile_rows(ops, s->R, lim.k[r], ops->batch_words_per_lane);
         s->HY[r] = (lim.k[r] + s->R - 1) / s->R * s->R;
         if (s->TH[r] - 2 * s->HY[r] <= 0) {
             destroy_all(s);
@@ -397,7 +399,7 @@ int cellato_server_iterate(cellato_server_t s, int* active) {
     std::vector<launch_rec> launches;
     for (int rule = 0; rule < CELLATO_RULE_COUNT; ++rule) {
         const rule_ops* ops = ops_of(rule);
-        const int effW = 32 * ops->temporal_words_per_lane - 2, effH = s->TH[rule] - 2 * s->HY[rule];
+        const int effW = 32 * ops->batch_words_per_lane - 2, effH = s->TH[rule] - 2 * s->HY[rule];
         for (const auto& round : plan.rounds[rule]) {
             const int first = (int)items.size();
             for (const sv::round_entry& en : round) {

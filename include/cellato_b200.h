@@ -320,7 +320,7 @@ typedef struct {
     int layout;                       /* cellato_layout */
     int word_bits;                    /* 32 or 64 */
     unsigned long long hbm_cap_bytes; /* resident plane bytes; 0: 80% of the device's memory */
-    int tile_budget;                  /* temporal tiles per round over all active requests; 0: 16 per SM */
+    int tile_budget;                  /* temporal tiles per round over all active requests; 0: 32 per SM */
     int chunk_rounds;                 /* rounds per request per iteration; 0: 4 */
     int max_inflight;                 /* iterations queued on the device at once; 0: 2 */
     int k_per_rule[10];               /* temporal depth per rule, 1..32; 0: 16 */
