@@ -23,7 +23,7 @@ from . import lib
 # k = 1 (one step per launch through a shared-memory tile), which for rules with
 # many planes or long networks reaches more of the HBM roofline.
 SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1)) + tuple(
-    ("temporal", 1, th, loop) for th in (0, 96, 128) for loop in (1, 2))
+    ("temporal", 1, th, loop, width) for th in (0, 96, 128, 192) for loop in (1, 2) for width in (0, 1))
 # (mode, k, tile_rows, row loop, words per lane); words per lane as
 # cellato_set_temporal_width (0 = the rule's default; 1 differs from it only for
 # rules of up to three planes, and is skipped for the others)
@@ -47,7 +47,7 @@ def cache_path() -> str:
 
 
 def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
-    return f"v6/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+    return f"v7/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
 
 
 def _load_file() -> dict:
