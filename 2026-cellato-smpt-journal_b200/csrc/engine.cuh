@@ -596,9 +596,9 @@ __global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, p
 // rolling window keeps the old value of the row above in registers, the row
 // below is read before it is overwritten, and horizontal neighbours come from
 // lane shuffles of registers, so no lane ever reads a word another lane writes
-// within a step.  Only the
-// two rows bordering a band belong to other warps: they are read before the
-// first barrier of the step and every write happens after it.
+// within a step.  Only the two rows bordering a band belong to other warps:
+// they are read before the first barrier of the step and every write happens
+// after it.
 // HOIST selects the row loop: true reads the three input rows of each 3-row
 // trip before the trip's writes; false reads each row just before the row
 // above it is evaluated.  Both compute the same values; which is faster
