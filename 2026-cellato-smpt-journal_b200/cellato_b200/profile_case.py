@@ -24,7 +24,9 @@ def main() -> None:
     ap.add_argument("--layout", default="tiled_bit_planes", choices=list(lib.LAYOUTS))
     ap.add_argument("--word-bits", type=int, default=64)
     ap.add_argument("--size", type=int, default=16384)
-    ap.add_argument("--mode", default="temporal", choices=["simple", "temporal"])
+    ap.add_argument("--mode", default="temporal", choices=["simple", "temporal", "ops"],
+                    help="ops: the whole-grid operations (checksum, diff, random fill, packing, bit_array "
+                         "conversion), each run --launches times")
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--loop", type=int, default=0, help="temporal row loop (cellato_set_temporal_variant)")
@@ -34,6 +36,8 @@ def main() -> None:
     a = ap.parse_args()
 
     r = lib.rule_id(a.rule)
+    if a.mode == "ops":
+        return ops(a, r)
     lib.set_temporal_variant(a.loop)
     lib.set_temporal_width(a.width)
     nb = lib.rule_planes(r)
@@ -61,6 +65,49 @@ def main() -> None:
                       "mode": a.mode, "k": k, "ms_per_launch": round(ms, 4),
                       "gcups": round(X * Y * k / (ms * 1e-3) / 1e9, 1),
                       "algorithmic_bytes_per_launch": 2 * nb * X * Y // 8}))
+
+
+def ops(a, r) -> None:
+    """Each whole-grid operation --launches times after one warm-up, with its
+    CUDA-event time and algorithmic bytes (what it must read and write)."""
+    nb = lib.rule_planes(r)
+    layout = lib.LAYOUTS[a.layout]
+    X = Y = a.size
+    pb = X * Y // 8
+    p, q = DevicePlanes(nb, X, Y), DevicePlanes(nb, X, Y)
+    th = inputs.thresholds(inputs.REFERENCE_DENSITY[inputs.RULES[r]])
+    cells = torch.empty((Y, X), dtype=torch.uint8, device="cuda")
+    sums = torch.zeros(16, dtype=torch.int64, device="cuda")
+    count = torch.zeros(1, dtype=torch.int64, device="cuda")
+    aw = 64
+    arr = torch.empty(lib.load().cellato_bit_array_bytes(nb, aw, X, Y), dtype=torch.uint8, device="cuda")
+    jobs = {
+        "fill_random": (lambda: lib.fill_random(layout, a.word_bits, nb, p.ptrs, X, Y, 7, th), nb * pb),
+        "checksum": (lambda: lib.checksum(r, layout, a.word_bits, p.ptrs, X, Y, sums.data_ptr()), nb * pb),
+        "diff_cells": (lambda: lib.diff_cells(nb, p.ptrs, q.ptrs, pb, count.data_ptr()), 2 * nb * pb),
+        "unpack_cells": (lambda: lib.unpack_cells(layout, a.word_bits, nb, p.ptrs, X, Y, cells.data_ptr()),
+                         nb * pb + X * Y),
+        "pack_cells": (lambda: lib.pack_cells(layout, a.word_bits, nb, cells.data_ptr(), X, Y, q.ptrs),
+                       nb * pb + X * Y),
+        "planes_to_bit_array": (lambda: lib.planes_to_bit_array(nb, layout, a.word_bits, p.ptrs, X, Y, aw,
+                                                                arr.data_ptr()), nb * pb + arr.numel()),
+        "bit_array_to_planes": (lambda: lib.bit_array_to_planes(nb, aw, arr.data_ptr(), X, Y, layout, a.word_bits,
+                                                                q.ptrs), nb * pb + arr.numel()),
+    }
+    out = {}
+    for name, (fn, byt) in jobs.items():
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.launches):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.launches
+        out[name] = {"ms": round(ms, 4), "algorithmic_bytes": byt, "gbs": round(byt / (ms * 1e-3) / 1e9, 1)}
+    print(json.dumps({"rule": inputs.RULES[r], "layout": a.layout, "word_bits": a.word_bits, "size": a.size,
+                      "ops": out}))
 
 
 if __name__ == "__main__":

@@ -33,9 +33,9 @@ namespace {
 
 constexpr int BA_WARPS = 8;
 
-template <int LAYOUT, typename AW>
+template <int LAYOUT, typename AW, int NB>
 __global__ void __launch_bounds__(BA_WARPS * 32) bit_array_to_planes_kernel(const AW* __restrict__ arr, int X,
-                                                                            int Xw, int nbands, int nb, int cpw,
+                                                                            int Xw, int nbands, int cpw,
                                                                             plane_set out) {
     constexpr int R = band_rows<LAYOUT>();
     const int lane = threadIdx.x & 31;
@@ -43,24 +43,24 @@ __global__ void __launch_bounds__(BA_WARPS * 32) bit_array_to_planes_kernel(cons
     if (w >= (long long)nbands * Xw) return;  // whole warp exits together
     const int b = (int)(w / Xw), gx = (int)(w % Xw);
     const long long row_words = X / cpw;
-    const AW mask = (AW(1) << nb) - 1;
+    const AW mask = (AW(1) << NB) - 1;
     const int x = 32 * gx + lane;
-    const int wi = x / cpw, off = (x % cpw) * nb;
-    word bits[R][MAX_PLANES];
+    const int wi = x / cpw, off = (x % cpw) * NB;
+    word bits[R][NB];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const long long y = (long long)b * R + r;
         const int idx = (int)((arr[y * row_words + wi] >> off) & mask);
 #pragma unroll
-        for (int p = 0; p < MAX_PLANES; ++p) bits[r][p] = __ballot_sync(0xffffffffu, (idx >> p) & 1);
+        for (int p = 0; p < NB; ++p) bits[r][p] = __ballot_sync(0xffffffffu, (idx >> p) & 1);
     }
-    if (lane < nb) {
+    if (lane < NB) {
         word rows[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             word v = 0;
 #pragma unroll
-            for (int p = 0; p < MAX_PLANES; ++p) v = (p == lane) ? bits[r][p] : v;
+            for (int p = 0; p < NB; ++p) v = (p == lane) ? bits[r][p] : v;
             rows[r] = v;
         }
         store_word_rows<LAYOUT>(out.p[lane], Xw, b, gx, rows);
@@ -134,7 +134,11 @@ void launch_to_planes(const AW* arr, int X, int Y, int nb, int cpw, const plane_
     const int Xw = X / 32, nbands = Y / R;
     const long long warps = (long long)nbands * Xw;
     const int blocks = (int)((warps + BA_WARPS - 1) / BA_WARPS);
-    if (blocks > 0) bit_array_to_planes_kernel<LAYOUT, AW><<<blocks, BA_WARPS * 32, 0, s>>>(arr, X, Xw, nbands, nb, cpw, ps);
+    if (blocks > 0)
+        dispatch_planes(nb, [&](auto c) {
+            bit_array_to_planes_kernel<LAYOUT, AW, decltype(c)::value>
+                <<<blocks, BA_WARPS * 32, 0, s>>>(arr, X, Xw, nbands, cpw, ps);
+        });
 }
 
 template <int LAYOUT, typename AW>

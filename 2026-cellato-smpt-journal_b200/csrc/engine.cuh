@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "b200/lower.cuh"
 
@@ -28,6 +29,18 @@ namespace cellato::b200 {
 enum : int { LAYOUT_LINEAR = 0, LAYOUT_TILED4 = 1, LAYOUT_TILED8 = 2 };
 
 constexpr int MAX_PLANES = 8;
+
+// Calls f(std::integral_constant<int, nb>{}) for a runtime plane count 1..MAX_PLANES,
+// so that per-plane loops in kernels run exactly nb times.
+template <int NB = 1, class F>
+inline void dispatch_planes(int nb, F&& f) {
+    if constexpr (NB <= MAX_PLANES) {
+        if (nb == NB)
+            f(std::integral_constant<int, NB>{});
+        else
+            dispatch_planes<NB + 1>(nb, f);
+    }
+}
 
 struct plane_set {
     word* p[MAX_PLANES];

@@ -148,8 +148,8 @@ __device__ __forceinline__ uint32_t splitmix_upper(unsigned long long seed, unsi
 
 // One warp per (band, linear word), lane = cell, one ballot per plane and row
 // (the layout of the packing kernel).
-template <int LAYOUT>
-__global__ void __launch_bounds__(OPS_WARPS * 32) fill_random_kernel(int X, int Xw, int nbands, int nb,
+template <int LAYOUT, int NB>
+__global__ void __launch_bounds__(OPS_WARPS * 32) fill_random_kernel(int X, int Xw, int nbands,
                                                                      unsigned long long seed, random_thresholds th,
                                                                      plane_set out) {
     constexpr int R = band_rows<LAYOUT>();
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(OPS_WARPS * 32) fill_random_kernel(int X, int 
     const long long w = (long long)blockIdx.x * OPS_WARPS + (threadIdx.x >> 5);
     if (w >= (long long)nbands * Xw) return;  // whole warp exits together
     const int b = (int)(w / Xw), gx = (int)(w % Xw);
-    word bits[R][MAX_PLANES];
+    word bits[R][NB];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const unsigned long long n = (unsigned long long)(b * R + r) * X + 32 * gx + lane;
@@ -165,15 +165,15 @@ __global__ void __launch_bounds__(OPS_WARPS * 32) fill_random_kernel(int X, int 
         int idx = 0;
         for (int i = 0; i < th.n; ++i) idx += (u >= th.t[i]) ? 1 : 0;
 #pragma unroll
-        for (int p = 0; p < MAX_PLANES; ++p) bits[r][p] = __ballot_sync(0xffffffffu, (idx >> p) & 1);
+        for (int p = 0; p < NB; ++p) bits[r][p] = __ballot_sync(0xffffffffu, (idx >> p) & 1);
     }
-    if (lane < nb) {
+    if (lane < NB) {
         word rows[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             word v = 0;
 #pragma unroll
-            for (int p = 0; p < MAX_PLANES; ++p) v = (p == lane) ? bits[r][p] : v;
+            for (int p = 0; p < NB; ++p) v = (p == lane) ? bits[r][p] : v;
             rows[r] = v;
         }
         store_word_rows<LAYOUT>(out.p[lane], Xw, b, gx, rows);
@@ -306,17 +306,20 @@ int enqueue_fill_random(int layout, int word_bits, int nb, const plane_set& ps, 
     const long long warps = (long long)nbands * Xw;
     const int blocks = (int)((warps + OPS_WARPS - 1) / OPS_WARPS);
     if (blocks > 0) {
-        switch (internal) {
-            case LAYOUT_LINEAR:
-                fill_random_kernel<LAYOUT_LINEAR><<<blocks, OPS_WARPS * 32, 0, s>>>(X, Xw, nbands, nb, seed, th, ps);
-                break;
-            case LAYOUT_TILED4:
-                fill_random_kernel<LAYOUT_TILED4><<<blocks, OPS_WARPS * 32, 0, s>>>(X, Xw, nbands, nb, seed, th, ps);
-                break;
-            case LAYOUT_TILED8:
-                fill_random_kernel<LAYOUT_TILED8><<<blocks, OPS_WARPS * 32, 0, s>>>(X, Xw, nbands, nb, seed, th, ps);
-                break;
-        }
+        dispatch_planes(nb, [&](auto c) {
+            constexpr int NB = decltype(c)::value;
+            switch (internal) {
+                case LAYOUT_LINEAR:
+                    fill_random_kernel<LAYOUT_LINEAR, NB><<<blocks, OPS_WARPS * 32, 0, s>>>(X, Xw, nbands, seed, th, ps);
+                    break;
+                case LAYOUT_TILED4:
+                    fill_random_kernel<LAYOUT_TILED4, NB><<<blocks, OPS_WARPS * 32, 0, s>>>(X, Xw, nbands, seed, th, ps);
+                    break;
+                case LAYOUT_TILED8:
+                    fill_random_kernel<LAYOUT_TILED8, NB><<<blocks, OPS_WARPS * 32, 0, s>>>(X, Xw, nbands, seed, th, ps);
+                    break;
+            }
+        });
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CELLATO_OK : cuda_fail(e, "random fill launch");

@@ -23,37 +23,37 @@ namespace {
 
 constexpr int PACK_WARPS = 8;
 
-template <int LAYOUT>
+template <int LAYOUT, int NB>
 __global__ void __launch_bounds__(PACK_WARPS * 32) pack_kernel(const uint8_t* __restrict__ cells, int X, int Xw,
-                                                               int nbands, int nb, plane_set out) {
+                                                               int nbands, plane_set out) {
     constexpr int R = band_rows<LAYOUT>();
     const int lane = threadIdx.x & 31;
     const long long w = (long long)blockIdx.x * PACK_WARPS + (threadIdx.x >> 5);
     if (w >= (long long)nbands * Xw) return;  // whole warp exits together
     const int b = (int)(w / Xw), gx = (int)(w % Xw);
-    word bits[R][MAX_PLANES];
+    word bits[R][NB];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const uint8_t c = cells[(size_t)(b * R + r) * X + 32 * gx + lane];
 #pragma unroll
-        for (int p = 0; p < MAX_PLANES; ++p) bits[r][p] = __ballot_sync(0xffffffffu, (c >> p) & 1);
+        for (int p = 0; p < NB; ++p) bits[r][p] = __ballot_sync(0xffffffffu, (c >> p) & 1);
     }
     // lane p stores plane p
-    if (lane < nb) {
+    if (lane < NB) {
         word rows[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             word v = 0;
 #pragma unroll
-            for (int p = 0; p < MAX_PLANES; ++p) v = (p == lane) ? bits[r][p] : v;
+            for (int p = 0; p < NB; ++p) v = (p == lane) ? bits[r][p] : v;
             rows[r] = v;
         }
         store_word_rows<LAYOUT>(out.p[lane], Xw, b, gx, rows);
     }
 }
 
-template <int LAYOUT>
-__global__ void __launch_bounds__(PACK_WARPS * 32) unpack_kernel(plane_set in, int X, int Xw, int nbands, int nb,
+template <int LAYOUT, int NB>
+__global__ void __launch_bounds__(PACK_WARPS * 32) unpack_kernel(plane_set in, int X, int Xw, int nbands,
                                                                  uint8_t* __restrict__ cells) {
     constexpr int R = band_rows<LAYOUT>();
     const int lane = threadIdx.x & 31;
@@ -63,14 +63,14 @@ __global__ void __launch_bounds__(PACK_WARPS * 32) unpack_kernel(plane_set in, i
     word mine[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) mine[r] = 0;
-    if (lane < nb) load_word_rows<LAYOUT>(in.p[lane], Xw, b, gx, mine);
+    if (lane < NB) load_word_rows<LAYOUT>(in.p[lane], Xw, b, gx, mine);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         uint32_t v = 0;
 #pragma unroll
-        for (int p = 0; p < MAX_PLANES; ++p) {
+        for (int p = 0; p < NB; ++p) {
             const word pw = __shfl_sync(0xffffffffu, mine[r], p);
-            if (p < nb) v |= ((pw >> lane) & 1u) << p;
+            v |= ((pw >> lane) & 1u) << p;
         }
         cells[(size_t)(b * R + r) * X + 32 * gx + lane] = (uint8_t)v;
     }
@@ -103,12 +103,15 @@ int cellato_pack_cells(int layout, int word_bits, int nb, const uint8_t* cells, 
     const long long warps = (long long)nbands * Xw;
     const dim3 grid((unsigned)((warps + PACK_WARPS - 1) / PACK_WARPS)), block(PACK_WARPS * 32);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (R == 1)
-        pack_kernel<LAYOUT_LINEAR><<<grid, block, 0, s>>>(cells, x_cells, Xw, nbands, nb, ps);
-    else if (R == 4)
-        pack_kernel<LAYOUT_TILED4><<<grid, block, 0, s>>>(cells, x_cells, Xw, nbands, nb, ps);
-    else
-        pack_kernel<LAYOUT_TILED8><<<grid, block, 0, s>>>(cells, x_cells, Xw, nbands, nb, ps);
+    dispatch_planes(nb, [&](auto c) {
+        constexpr int NB = decltype(c)::value;
+        if (R == 1)
+            pack_kernel<LAYOUT_LINEAR, NB><<<grid, block, 0, s>>>(cells, x_cells, Xw, nbands, ps);
+        else if (R == 4)
+            pack_kernel<LAYOUT_TILED4, NB><<<grid, block, 0, s>>>(cells, x_cells, Xw, nbands, ps);
+        else
+            pack_kernel<LAYOUT_TILED8, NB><<<grid, block, 0, s>>>(cells, x_cells, Xw, nbands, ps);
+    });
     return cudaGetLastError() == cudaSuccess ? CELLATO_OK : CELLATO_ECUDA;
 }
 
@@ -122,12 +125,15 @@ int cellato_unpack_cells(int layout, int word_bits, int nb, const void* const* p
     const long long warps = (long long)nbands * Xw;
     const dim3 grid((unsigned)((warps + PACK_WARPS - 1) / PACK_WARPS)), block(PACK_WARPS * 32);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (R == 1)
-        unpack_kernel<LAYOUT_LINEAR><<<grid, block, 0, s>>>(ps, x_cells, Xw, nbands, nb, cells);
-    else if (R == 4)
-        unpack_kernel<LAYOUT_TILED4><<<grid, block, 0, s>>>(ps, x_cells, Xw, nbands, nb, cells);
-    else
-        unpack_kernel<LAYOUT_TILED8><<<grid, block, 0, s>>>(ps, x_cells, Xw, nbands, nb, cells);
+    dispatch_planes(nb, [&](auto c) {
+        constexpr int NB = decltype(c)::value;
+        if (R == 1)
+            unpack_kernel<LAYOUT_LINEAR, NB><<<grid, block, 0, s>>>(ps, x_cells, Xw, nbands, cells);
+        else if (R == 4)
+            unpack_kernel<LAYOUT_TILED4, NB><<<grid, block, 0, s>>>(ps, x_cells, Xw, nbands, cells);
+        else
+            unpack_kernel<LAYOUT_TILED8, NB><<<grid, block, 0, s>>>(ps, x_cells, Xw, nbands, cells);
+    });
     return cudaGetLastError() == cudaSuccess ? CELLATO_OK : CELLATO_ECUDA;
 }
 
