@@ -94,6 +94,9 @@ def ops(a, r) -> None:
         "bit_array_to_planes": (lambda: lib.bit_array_to_planes(nb, aw, arr.data_ptr(), X, Y, layout, a.word_bits,
                                                                 q.ptrs), nb * pb + arr.numel()),
     }
+    if X % (aw // nb):  # the bit_array layout needs whole words per row
+        jobs.pop("planes_to_bit_array")
+        jobs.pop("bit_array_to_planes")
     out = {}
     for name, (fn, byt) in jobs.items():
         fn()

@@ -54,39 +54,42 @@ struct random_thresholds {
     int n;
 };
 
-// Tile-sum accumulator of one thread: the running sum of the tile it last
-// touched, added to the CTA's shared sums when the tile changes.
+// Tile-sum accumulator of one thread: per term of the value polynomial, the
+// popcount total of the tile it last touched (32-bit: at most 32 cells per word
+// and fewer than 2^27 words per tile and thread); the weighted sum goes to the
+// CTA's shared sums when the tile changes.
+template <int NT>
 struct tile_acc {
     int key = -1;
-    long long sum = 0;
-    __device__ void add(int k, long long v, unsigned long long* sh) {
-        if (k != key) {
-            if (key >= 0 && sum) atomicAdd(&sh[key], (unsigned long long)sum);
-            key = k;
-            sum = 0;
+    unsigned cnt[NT] = {};
+    __device__ void flush(unsigned long long* sh, const checksum_terms& terms) {
+        if (key >= 0) {
+            long long v = 0;
+#pragma unroll
+            for (int i = 0; i < NT; ++i) v += terms.coef[i] * (long long)cnt[i];
+            if (v) atomicAdd(&sh[key], (unsigned long long)v);
         }
-        sum += v;
+#pragma unroll
+        for (int i = 0; i < NT; ++i) cnt[i] = 0;
     }
-    __device__ void flush(unsigned long long* sh) {
-        if (key >= 0 && sum) atomicAdd(&sh[key], (unsigned long long)sum);
-        key = -1;
-        sum = 0;
+    // adds the cells of one row word selected by `mask` to tile k
+    template <int NB>
+    __device__ void add(int k, const word (&P)[NB], word mask, const checksum_terms& terms, unsigned long long* sh) {
+        if (k != key) {
+            flush(sh, terms);
+            key = k;
+        }
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+            if (i >= terms.n) break;
+            word m = mask;
+            const unsigned sel = terms.planes[i];
+#pragma unroll
+            for (int p = 0; p < NB; ++p) m &= ((sel >> p) & 1u) ? P[p] : ~0u;
+            cnt[i] += __popc(m);
+        }
     }
 };
-
-// Sum of the state values of the cells of one row word selected by `mask`.
-template <int NB>
-__device__ __forceinline__ long long masked_value_sum(const word (&P)[NB], word mask, const checksum_terms& terms) {
-    long long v = 0;
-    for (int i = 0; i < terms.n; ++i) {
-        word m = mask;
-        const unsigned sel = terms.planes[i];
-#pragma unroll
-        for (int p = 0; p < NB; ++p) m &= ((sel >> p) & 1u) ? P[p] : ~0u;
-        v += terms.coef[i] * (long long)__popc(m);
-    }
-    return v;
-}
 
 // Each warp takes a contiguous run of (band, word) units, lane-interleaved, so
 // a thread's consecutive units are 32 words apart in the same rows and its
@@ -97,6 +100,7 @@ __global__ void __launch_bounds__(OPS_WARPS * 32) checksum_kernel(plane_set in, 
                                                                   checksum_terms terms,
                                                                   unsigned long long* __restrict__ out) {
     constexpr int R = band_rows<LAYOUT>();
+    constexpr int NT = (1 << NB) < MAX_TERMS ? (1 << NB) : MAX_TERMS;
     __shared__ unsigned long long sh[16];
     if (threadIdx.x < 16) sh[threadIdx.x] = 0;
     __syncthreads();
@@ -105,7 +109,7 @@ __global__ void __launch_bounds__(OPS_WARPS * 32) checksum_kernel(plane_set in, 
     const long long units = (long long)nbands * Xw;
     const long long u0 = warp * units_per_warp;
     const long long u1 = min(units, u0 + units_per_warp);
-    tile_acc acc;
+    tile_acc<NT> acc;
     for (long long u = u0 + lane; u < u1; u += 32) {
         const int b = (int)(u / Xw), gx = (int)(u % Xw);
         word rows[NB][R];
@@ -123,17 +127,17 @@ __global__ void __launch_bounds__(OPS_WARPS * 32) checksum_kernel(plane_set in, 
 #pragma unroll
             for (int p = 0; p < NB; ++p) P[p] = rows[p][r];
             if (whole) {
-                acc.add(ty * 4 + tx0, masked_value_sum<NB>(P, ~0u, terms), sh);
+                acc.template add<NB>(ty * 4 + tx0, P, ~0u, terms, sh);
             } else {
                 for (int tx = tx0; tx < 4 && tx * tw < x0 + 32; ++tx) {
                     const int lo = max(tx * tw - x0, 0), hi = min((tx + 1) * tw - x0, 32);
                     const word mask = (hi >= 32 ? ~0u : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
-                    acc.add(ty * 4 + tx, masked_value_sum<NB>(P, mask, terms), sh);
+                    acc.template add<NB>(ty * 4 + tx, P, mask, terms, sh);
                 }
             }
         }
     }
-    acc.flush(sh);
+    acc.flush(sh, terms);
     __syncthreads();
     if (threadIdx.x < 16 && sh[threadIdx.x]) atomicAdd(&out[threadIdx.x], sh[threadIdx.x]);
 }
@@ -245,8 +249,9 @@ void launch_checksum(const plane_set& ps, int X, int Y, const checksum_terms& te
     constexpr int R = band_rows<LAYOUT>();
     const int Xw = X / 32, nbands = Y / R;
     const long long units = (long long)nbands * Xw;
-    // about 16 warps per SM, each a contiguous run of whole 32-unit groups
-    const long long warps = 148LL * 16;
+    // about 64 warps per SM (enough loads in flight for HBM), each a
+    // contiguous run of whole 32-unit groups
+    const long long warps = 148LL * 64;
     long long per_warp = (units + warps - 1) / warps;
     per_warp = (per_warp + 31) / 32 * 32;
     const long long used = (units + per_warp - 1) / per_warp;
