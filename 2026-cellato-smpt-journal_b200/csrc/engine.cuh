@@ -622,7 +622,9 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
     constexpr int R = band_rows<LAYOUT>();
     constexpr int TW = 32 * V;  // tile width in words
     using feat = typename Net::feat;
-    extern __shared__ __align__(16) word tile[];  // [NB][TH][TW]
+    // [TH][NB][TW]: a row's planes are adjacent, so one base address per row
+    // reaches all of them through constant offsets
+    extern __shared__ __align__(16) word tile[];
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -632,7 +634,7 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
     const int y0 = by * effH;  // first output row
     const int Yb = Y / R;
 
-    auto at = [&](int p, int r, int s) -> word& { return tile[((size_t)p * TH + r) * TW + s]; };
+    auto at = [&](int p, int r, int s) -> word& { return tile[((size_t)r * NB + p) * TW + s]; };
 
     // ---- load the tile (rows wrap on the torus; words wrap per word)
     for (int band = warp; band < TH / R; band += WARPS) {
