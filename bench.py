@@ -49,8 +49,8 @@ CPU_SAMPLE_SIZE = 2048
 # per k stands for them.
 MEASURED_TRAFFIC = {
     ("wire", "temporal", 8, 16384): (84.97e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md"),
-    ("wire", "temporal", 16, 16384): (85.12e6, "profiles/temporal_kernel_wire_tiled64_16384_k16.md"),
-    ("excitable", "temporal", 16, 16384): (150.22e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
+    ("wire", "temporal", 16, 16384): (82.89e6, "profiles/temporal_kernel_wire_tiled64_16384_k16.md"),
+    ("excitable", "temporal", 16, 16384): (151.17e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
 }
 
 
