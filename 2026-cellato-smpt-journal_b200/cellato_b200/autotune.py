@@ -23,13 +23,13 @@ from . import lib
 # k = 1 (one step per launch through a shared-memory tile), which for rules with
 # many planes or long networks reaches more of the HBM roofline.
 SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1)) + tuple(
-    ("temporal", 1, th, loop, width) for th in (0, 96, 128, 192) for loop in (1, 2) for width in (0, 1))
+    ("temporal", 1, th, loop, width) for th in (0, 96, 128, 192) for loop in (1, 2) for width in (1, 2))
 # (mode, k, tile_rows, row loop, words per lane); words per lane as
-# cellato_set_temporal_width (0 = the rule's default; 1 differs from it only for
-# rules of up to three planes, and is skipped for the others)
+# cellato_set_temporal_width (1 or 2; two words per lane exist only for rules of
+# up to three planes, and are skipped for the others)
 DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2),) + tuple(
     ("temporal", k, th, loop, width) for k in (4, 6, 8, 12, 16, 24) for th in (0, 96, 128, 160, 192, 256, 320)
-    for loop in (1, 2) for width in (0, 1))
+    for loop in (1, 2) for width in (1, 2))
 _VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2}
 
 _lock = threading.Lock()
@@ -47,7 +47,7 @@ def cache_path() -> str:
 
 
 def _key(rule: int, layout: int, word_bits: int, X: int, Y: int, device_name: str) -> str:
-    return f"v7/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
+    return f"v8/{rule}/{layout}/{word_bits}/{size_class(X, Y)}/{device_name}"
 
 
 def _load_file() -> dict:
@@ -120,8 +120,8 @@ def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, 
         width = cand[4] if len(cand) > 4 else 0
         if th and th - 2 * ((k + 7) // 8 * 8) < 8:
             continue  # the halos would leave no interior
-        if width == 1 and lib.rule_planes(rule) > 3:
-            continue  # one word per lane is already these rules' default
+        if width == 2 and lib.rule_planes(rule) > 3:
+            continue  # these rules have only the one-word-per-lane kernel
         choice = {"mode": mode, "k": k, "tile_rows": th, "loop": loop, "width": width}
         steps = max(burst_steps, 2 * k) // k * k
         try:

@@ -90,18 +90,24 @@ int max_optin_smem() {
     return v;
 }
 
-// Default tile height for k fused steps: 128 interior rows plus the two halos
-// (HY = ceil(k/R)*R rows each), at most what still lets two CTAs share an SM.
+// Default tile height for k fused steps: `interior` rows plus the two halos
+// (HY = ceil(k/R)*R rows each).  The cap is the tallest tile that lets three
+// CTAs share an SM when that still leaves 96 interior rows, otherwise two.
 // Taller tiles waste less on halos but leave fewer CTAs for the 148 SMs and
-// fewer resident warps per SM; measured on B200 at 16384^2 over the ten rules,
-// this height is within a few percent of the best single height per rule.
-int default_tile_rows(const rule_ops* ops, int R, int k, int V) {
+// fewer resident warps per SM.  Single grids use 224 interior rows for rules
+// of two or more planes (with one word per lane, on B200 at 16384^2 and
+// k = 16, 3-13% faster than two words per lane and 128 rows for the seven
+// such rules, both layouts) and 128 for one-plane rules (224 is 2-7% slower
+// there); batches, with their many small grids, use 128.
+int default_tile_rows(const rule_ops* ops, int R, int k, int V, int interior) {
     const int row_bytes = ops->planes * 32 * V * 4;
     const int q = std::max(ops->temporal_warps, R);
     const int HY = (std::max(1, k) + R - 1) / R * R;
+    const int three_per_sm = (75 * 1024) / row_bytes / q * q;
     const int two_per_sm = (113 * 1024) / row_bytes / q * q;
-    const int want = (2 * HY + 128 + q - 1) / q * q;
-    return std::min(want, std::max(two_per_sm, (2 * HY + q) / q * q));
+    const int cap = three_per_sm >= 2 * HY + 96 ? three_per_sm : two_per_sm;
+    const int want = (2 * HY + interior + q - 1) / q * q;
+    return std::min(want, std::max(cap, (2 * HY + q) / q * q));
 }
 
 }  // namespace cellato::b200::capi
@@ -276,7 +282,7 @@ int cellato_run_temporal(int rule, int layout, int word_bits, void* const* plane
     const int R = band_height(layout, word_bits);
     const int q = std::max(ops->temporal_warps, R);
     const int V = ops->temporal_v_now();
-    const int TH = tile_rows > 0 ? tile_rows : default_tile_rows(ops, R, k, V);
+    const int TH = tile_rows > 0 ? tile_rows : default_tile_rows(ops, R, k, V, ops->planes == 1 ? 128 : 224);
     if (TH % q != 0)
         return fail(CELLATO_EINVAL, "temporal tile rows %d must be a multiple of %d", TH, q);
     const int row_bytes = ops->planes * 32 * V * 4;

@@ -17,7 +17,7 @@ int internal_layout(int layout, int word_bits);
 int band_height(int layout, int word_bits);
 int check_dims(int layout, int word_bits, int X, int Y);
 int make_sets(const rule_ops* ops, void* const* a, void* const* b, plane_set& pa, plane_set& pb);
-int default_tile_rows(const rule_ops* ops, int R, int k, int V);
+int default_tile_rows(const rule_ops* ops, int R, int k, int V, int interior = 128);
 // grid_ops.cu: stream-ordered checksum (16 device uint64) and random fill
 int enqueue_checksum(const rule_ops* ops, int layout, int word_bits, const plane_set& ps, int X, int Y,
                      unsigned long long* out, cudaStream_t s);

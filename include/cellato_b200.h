@@ -159,8 +159,8 @@ int cellato_set_simple_variant(int variant);
  * reference (one temporal kernel). */
 int cellato_set_temporal_variant(int variant);
 
-/* Words per lane of the temporal kernel (cellato_run_temporal): 0 = the rule's
- * default (2 for rules of up to three planes, else 1), 1 = one word per lane
+/* Words per lane of the temporal kernel (cellato_run_temporal): 0 = the
+ * library's default (2 for one-plane rules, else 1), 1 = one word per lane
  * (half the registers and shared memory per tile row, so more CTAs per SM),
  * 2 = two (rules of up to three planes; others use one).  Same results; the
  * tile is 32 x words-per-lane words wide, so default tile heights and

@@ -62,7 +62,7 @@ def checksum(rule, layout, p, X, Y):
 
 @pytest.mark.parametrize("rule,k,th,loop,width", [("wire", 8, 128, 1, 0), ("wire", 16, 0, 2, 0),
                                                   ("excitable", 16, 0, 2, 0), ("excitable", 8, 128, 1, 0),
-                                                  ("excitable", 16, 192, 2, 1), ("wire", 16, 192, 1, 1)])
+                                                  ("excitable", 16, 192, 2, 2), ("wire", 16, 192, 1, 1)])
 def test_config2_size_temporal_equals_single_step(cuda, rule, k, th, loop, width):
     import torch
     r = lib.rule_id(rule)
