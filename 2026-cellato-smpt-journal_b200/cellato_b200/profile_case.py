@@ -24,9 +24,10 @@ def main() -> None:
     ap.add_argument("--layout", default="tiled_bit_planes", choices=list(lib.LAYOUTS))
     ap.add_argument("--word-bits", type=int, default=64)
     ap.add_argument("--size", type=int, default=16384)
-    ap.add_argument("--mode", default="temporal", choices=["simple", "temporal", "ops"],
+    ap.add_argument("--mode", default="temporal", choices=["simple", "temporal", "ops", "lop3"],
                     help="ops: the whole-grid operations (checksum, diff, random fill, packing, bit_array "
-                         "conversion), each run --launches times")
+                         "conversion), each run --launches times; lop3: the ALU-pipe rate kernel "
+                         "(cellato_lop3_rate: one warm-up and three timed launches)")
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--loop", type=int, default=0, help="temporal row loop (cellato_set_temporal_variant)")
@@ -36,6 +37,9 @@ def main() -> None:
     a = ap.parse_args()
 
     r = lib.rule_id(a.rule)
+    if a.mode == "lop3":
+        print(json.dumps({"lop3_lane_ops_per_s": lib.lop3_rate()}))
+        return
     if a.mode == "ops":
         return ops(a, r)
     lib.set_temporal_variant(a.loop)

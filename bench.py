@@ -53,6 +53,13 @@ MEASURED_TRAFFIC = {
     ("excitable", "temporal", 16, 16384): (151.17e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
 }
 
+# ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
+# temporal kernel configuration, from one ncu capture of that configuration
+# (summary in profiles/); keyed by (rule, layout, k, tile_rows, row loop, words
+# per lane, size).  Each configuration is timed live and set against the ALU
+# pipe's measured rate (cellato_lop3_rate) for the compute roofline.
+MEASURED_ALU = {}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -493,6 +500,35 @@ def our_arm(args, rank: int, world: int):
         g["a"].buf.copy_(g["init"].buf)
     torch.cuda.synchronize()
 
+    # ---- compute roofline of the temporal kernels: ALU-pipe instructions per
+    # launch (ncu count of the configuration) over the live launch time, against
+    # the ALU pipe's measured LOP3 rate on this device
+    alu = {"bound": "alu", "unit": "Gop/s (32-bit lane operations)",
+           "peak": round(lib.lop3_rate(sp) / 1e9, 1),
+           "peak_source": "measured live: cellato_lop3_rate (independent lop3.b32 chains, full occupancy)",
+           "kernels": {}}
+    for key, (count, src) in MEASURED_ALU.items():
+        a, lay, k, th, loop, width, size = key
+        if a not in grids or lay != LAYOUT or size != args.size:
+            continue
+        g = grids[a]
+        c = {"mode": "temporal", "k": k, "tile_rows": th, "loop": loop, "width": width}
+        nl = 8
+        autotune.run(c, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, 2 * k, sp)
+        e0.record(stream)
+        autotune.run(c, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, nl * k, sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        msl = e0.elapsed_time(e1) / nl
+        ach = count * 32 / (msl * 1e-3) / 1e9
+        alu["kernels"][a] = {"kernel": describe_choice(c),
+                             "timed_choice": all(g["choice"].get(n) == v for n, v in c.items()),
+                             "alu_warp_insts_per_launch": count, "ms_per_launch": round(msl, 4),
+                             "achieved": round(ach, 1), "frac": round(ach / alu["peak"], 4),
+                             "alu_ops_per_cell_step": round(count * 32 / (X * Y * k), 2), "source": src}
+        g["a"].buf.copy_(g["init"].buf)
+    torch.cuda.synchronize()
+
     # ---- roofline of the dominant kernel (the automaton with the most time)
     dom = max(AUTOMATA, key=lambda a: sum(per[a]))
     g = grids[dom]
@@ -540,6 +576,7 @@ def our_arm(args, rank: int, world: int):
         "gpu_launches": n_launch,
         "roofline": roof,
         "single_step_roofline": {"peak_gbs": peaks["hbm_gbs"], "peak_source": peaks["source"], **single},
+        "alu_roofline": alu,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
     }

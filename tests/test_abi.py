@@ -13,7 +13,7 @@ from conftest import ROOT, RULES
 
 def declared_functions():
     text = open(os.path.join(ROOT, "include", "cellato_b200.h")).read()
-    return sorted(set(re.findall(r"\b(cellato_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(cellato_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():
