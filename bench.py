@@ -58,7 +58,12 @@ MEASURED_TRAFFIC = {
 # (summary in profiles/); keyed by (rule, layout, k, tile_rows, row loop, words
 # per lane, size).  Each configuration is timed live and set against the ALU
 # pipe's measured rate (cellato_lop3_rate) for the compute roofline.
-MEASURED_ALU = {}
+MEASURED_ALU = {
+    ("wire", 1, 16, 256, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md"),
+    ("excitable", 1, 16, 192, 2, 1, 16384): (70869600, "profiles/alu_pipe_temporal_kernels.md"),
+    ("cyclic", 0, 12, 160, 2, 1, 32768): (1234003680, "profiles/alu_pipe_temporal_kernels.md"),
+    ("fluid", 0, 16, 128, 2, 1, 32768): (322018480, "profiles/alu_pipe_temporal_kernels.md"),
+}
 
 
 def parse():
