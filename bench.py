@@ -56,13 +56,13 @@ MEASURED_TRAFFIC = {
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
 # temporal kernel configuration, from one ncu capture of that configuration
 # (summary in profiles/); keyed by (rule, layout, k, tile_rows, row loop, words
-# per lane, size).  Each configuration is timed live and set against the ALU
+# per lane, size), tile_rows 0 being the library's default height.  Each configuration is timed live and set against the ALU
 # pipe's measured rate (cellato_lop3_rate) for the compute roofline.
 MEASURED_ALU = {
-    ("wire", 1, 16, 256, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md"),
-    ("excitable", 1, 16, 192, 2, 1, 16384): (70869600, "profiles/alu_pipe_temporal_kernels.md"),
-    ("cyclic", 0, 12, 160, 2, 1, 32768): (1234003680, "profiles/alu_pipe_temporal_kernels.md"),
-    ("fluid", 0, 16, 128, 2, 1, 32768): (322018480, "profiles/alu_pipe_temporal_kernels.md"),
+    ("wire", 1, 16, 0, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md"),
+    ("excitable", 1, 16, 0, 2, 1, 16384): (70207344, "profiles/alu_pipe_temporal_kernels.md"),
+    ("cyclic", 0, 16, 0, 2, 1, 32768): (1664571440, "profiles/alu_pipe_temporal_kernels.md"),
+    ("fluid", 0, 16, 0, 2, 1, 32768): (312104380, "profiles/alu_pipe_temporal_kernels.md"),
 }
 
 
