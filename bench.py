@@ -51,6 +51,8 @@ MEASURED_TRAFFIC = {
     ("wire", "temporal", 8, 16384): (84.97e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md"),
     ("wire", "temporal", 16, 16384): (82.89e6, "profiles/temporal_kernel_wire_tiled64_16384_k16.md"),
     ("excitable", "temporal", 16, 16384): (151.17e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
+    ("cyclic", "temporal", 16, 32768): (1295.33e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md"),
+    ("fluid", "temporal", 16, 32768): (1028.18e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md"),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
