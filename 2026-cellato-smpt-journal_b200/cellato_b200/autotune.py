@@ -18,14 +18,14 @@ import threading
 from . import lib
 
 # (mode, k[, tile_rows[, row loop]]); tile_rows 0 = the library's default height
-# for k; row loop as cellato_set_temporal_variant (0 = default)
+# for k; row loop as cellato_tune.row_loop (0 = default)
 # Single-step candidates: the two single-step kernels and the temporal kernel at
 # k = 1 (one step per launch through a shared-memory tile), which for rules with
 # many planes or long networks reaches more of the HBM roofline.
 SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1)) + tuple(
     ("temporal", 1, th, loop, width) for th in (0, 96, 128, 192) for loop in (1, 2) for width in (1, 2))
 # (mode, k, tile_rows, row loop, words per lane); words per lane as
-# cellato_set_temporal_width (1 or 2; two words per lane exist only for rules of
+# cellato_tune.words_per_lane (1 or 2; two words per lane exist only for rules of
 # up to three planes, and are skipped for the others)
 DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2),) + tuple(
     ("temporal", k, th, loop, width) for k in (4, 6, 8, 12, 16, 24) for th in (0, 96, 128, 160, 192, 256, 320)
@@ -75,19 +75,11 @@ def run(choice: dict, rule: int, layout: int, word_bits: int, planes_a, planes_b
         steps: int, stream: int = 0) -> int:
     """Run `steps` steps with a tuned choice; returns 1 if the result is in planes_b."""
     if choice["mode"] in _VARIANT:
-        lib.set_simple_variant(_VARIANT[choice["mode"]])
-        try:
-            return lib.run_simple(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, stream)
-        finally:
-            lib.set_simple_variant(0)
-    lib.set_temporal_variant(choice.get("loop", 0))
-    lib.set_temporal_width(choice.get("width", 0))
-    try:
-        return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
-                                choice.get("tile_rows", 0), stream)
-    finally:
-        lib.set_temporal_variant(0)
-        lib.set_temporal_width(0)
+        return lib.run_simple(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, stream,
+                              simple_kernel=_VARIANT[choice["mode"]])
+    return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
+                            choice.get("tile_rows", 0), stream, row_loop=choice.get("loop", 0),
+                            words_per_lane=choice.get("width", 0))
 
 
 def tune(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, candidates=DEFAULT_CANDIDATES,

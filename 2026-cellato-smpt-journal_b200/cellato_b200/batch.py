@@ -23,12 +23,9 @@ class Batch:
                 arr[i].planes_a[p] = ptr
             for p, ptr in enumerate(pb):
                 arr[i].planes_b[p] = ptr
-        ks = None
-        if k_per_rule is not None:
-            ks = (ctypes.c_int * 10)(*[int(k_per_rule.get(r, 0)) if isinstance(k_per_rule, dict) else int(k_per_rule[r])
-                                      for r in range(10)])
+        ks, nk = lib.k_array(k_per_rule)
         h = ctypes.c_void_p()
-        lib.check(L.cellato_batch_create(layout, word_bits, arr, len(grids), ks, ctypes.byref(h)))
+        lib.check(L.cellato_batch_create(layout, word_bits, arr, len(grids), ks, nk, ctypes.byref(h)))
         self._h = h
         self.n = len(grids)
 
@@ -70,9 +67,7 @@ def run_noalloc(layout: int, word_bits: int, grids, k_per_rule=None, stream: int
             arr[i].planes_a[p] = ptr
         for p, ptr in enumerate(pb):
             arr[i].planes_b[p] = ptr
-    ks = None
-    if k_per_rule is not None:
-        ks = (ctypes.c_int * 10)(*[int(k_per_rule.get(r, 0)) for r in range(10)])
+    ks, nk = lib.k_array(k_per_rule)
     flags = (ctypes.c_int * max(1, len(grids)))()
-    lib.check(L.cellato_batch_run_noalloc(layout, word_bits, arr, len(grids), ks, stream, flags))
+    lib.check(L.cellato_batch_run_noalloc(layout, word_bits, arr, len(grids), ks, nk, stream, flags))
     return [flags[i] for i in range(len(grids))]

@@ -23,12 +23,12 @@ LAYOUTS = {"bit_planes": LAYOUT_BIT_PLANES, "tiled_bit_planes": LAYOUT_TILED_BIT
 # Every symbol include/cellato_b200.h declares (checked by the CPU tests).
 EXPORTED = [
     "cellato_version", "cellato_last_error", "cellato_rule_from_name", "cellato_rule_name",
-    "cellato_rule_planes", "cellato_rule_states", "cellato_plane_bytes", "cellato_check_dims",
+    "cellato_rule_planes", "cellato_rule_states", "cellato_rule_count", "cellato_rule_register",
+    "cellato_plane_bytes", "cellato_check_dims",
     "cellato_planes_alloc", "cellato_planes_free", "cellato_planes_upload", "cellato_planes_download",
     "cellato_pack_cells", "cellato_unpack_cells",
     "cellato_run_simple", "cellato_run_temporal", "cellato_temporal_max_tile_rows",
-    "cellato_device_wait_timeouts", "cellato_set_simple_variant", "cellato_set_temporal_variant",
-    "cellato_set_temporal_width",
+    "cellato_device_wait_timeouts",
     "cellato_batch_create", "cellato_batch_launch", "cellato_batch_result_in_b", "cellato_batch_info",
     "cellato_batch_destroy", "cellato_batch_run_noalloc",
     "cellato_checksum", "cellato_rule_state_value", "cellato_fill_random", "cellato_diff_cells",
@@ -46,6 +46,16 @@ class CellatoError(RuntimeError):
         self.status = status
 
 
+BUILTIN_RULES = 10
+MAX_RULES = 256
+
+
+class Tune(ctypes.Structure):
+    """cellato_tune: per-call kernel choices (0 = the library's choice)."""
+    _fields_ = [("simple_kernel", ctypes.c_int), ("row_loop", ctypes.c_int), ("words_per_lane", ctypes.c_int),
+                ("tile_rows", ctypes.c_int)]
+
+
 class BatchGrid(ctypes.Structure):
     _fields_ = [("rule", ctypes.c_int), ("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int),
                 ("steps", ctypes.c_int), ("planes_a", ctypes.c_void_p * 8), ("planes_b", ctypes.c_void_p * 8)]
@@ -54,7 +64,7 @@ class BatchGrid(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("layout", ctypes.c_int), ("word_bits", ctypes.c_int), ("hbm_cap_bytes", ctypes.c_ulonglong),
                 ("tile_budget", ctypes.c_int), ("chunk_rounds", ctypes.c_int), ("max_inflight", ctypes.c_int),
-                ("k_per_rule", ctypes.c_int * 10)]
+                ("k_per_rule", ctypes.POINTER(ctypes.c_int)), ("n_k_per_rule", ctypes.c_int)]
 
 
 class ServerResult(ctypes.Structure):
@@ -93,16 +103,19 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cellato_planes_upload.argtypes = [ctypes.c_int, _PP, _PP, ctypes.c_size_t, _vp]
     lib.cellato_planes_download.argtypes = [ctypes.c_int, _PP, _PP, ctypes.c_size_t, _vp]
     i = ctypes.c_int
-    lib.cellato_run_simple.argtypes = [i, i, i, _PP, _PP, i, i, i, i, _vp, ctypes.POINTER(i)]
-    lib.cellato_run_temporal.argtypes = [i, i, i, _PP, _PP, i, i, i, i, i, i, _vp, ctypes.POINTER(i)]
-    lib.cellato_batch_create.argtypes = [i, i, ctypes.POINTER(BatchGrid), i, ctypes.POINTER(ctypes.c_int),
+    TP = ctypes.POINTER(Tune)
+    lib.cellato_run_simple.argtypes = [i, i, i, _PP, _PP, i, i, i, i, TP, _vp, ctypes.POINTER(i)]
+    lib.cellato_run_temporal.argtypes = [i, i, i, _PP, _PP, i, i, i, i, i, TP, _vp, ctypes.POINTER(i)]
+    lib.cellato_temporal_max_tile_rows.argtypes = [i, i, i, i]
+    lib.cellato_rule_register.argtypes = [_vp, ctypes.POINTER(i)]
+    lib.cellato_batch_create.argtypes = [i, i, ctypes.POINTER(BatchGrid), i, ctypes.POINTER(ctypes.c_int), i,
                                          ctypes.POINTER(ctypes.c_void_p)]
     lib.cellato_batch_launch.argtypes = [_vp, _vp]
     lib.cellato_batch_result_in_b.argtypes = [_vp, i, ctypes.POINTER(i)]
     lib.cellato_batch_info.argtypes = [_vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]
     lib.cellato_batch_destroy.argtypes = [_vp]
-    lib.cellato_batch_run_noalloc.argtypes = [i, i, ctypes.POINTER(BatchGrid), i, ctypes.POINTER(ctypes.c_int), _vp,
-                                              ctypes.POINTER(ctypes.c_int)]
+    lib.cellato_batch_run_noalloc.argtypes = [i, i, ctypes.POINTER(BatchGrid), i, ctypes.POINTER(ctypes.c_int), i,
+                                              _vp, ctypes.POINTER(ctypes.c_int)]
     lib.cellato_pack_cells.argtypes = [i, i, i, _vp, i, i, _PP, _vp]
     lib.cellato_unpack_cells.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
     u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -166,13 +179,38 @@ def rule_name(rule) -> str:
     return load().cellato_rule_name(rule_id(rule)).decode()
 
 
+def tune(simple_kernel: int = 0, row_loop: int = 0, words_per_lane: int = 0, tile_rows: int = 0) -> Tune:
+    return Tune(simple_kernel, row_loop, words_per_lane, tile_rows)
+
+
 def run_simple(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,
-               stream: int = 0) -> int:
-    """Returns 1 when the result ended in planes_b, else 0."""
+               stream: int = 0, simple_kernel: int = 0) -> int:
+    """Returns 1 when the result ended in planes_b, else 0.  simple_kernel as
+    cellato_tune (0 automatic, 1 register bands, 2 bulk-copy streaming)."""
     out = ctypes.c_int(0)
+    t = tune(simple_kernel=simple_kernel)
     check(load().cellato_run_simple(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),
-                                    X, Y, t0, steps, stream, ctypes.byref(out)))
+                                    X, Y, t0, steps, ctypes.byref(t), stream, ctypes.byref(out)))
     return out.value
+
+
+def rule_count() -> int:
+    return load().cellato_rule_count()
+
+
+def rule_register(ops_ptr: int) -> int:
+    """Registers a rule table (the address a custom_rule_ops<Config>() call
+    returned in a caller-built library) and returns its rule id."""
+    out = ctypes.c_int(-1)
+    check(load().cellato_rule_register(ops_ptr, ctypes.byref(out)))
+    return out.value
+
+
+def temporal_max_tile_rows(rule, layout: int, word_bits: int, words_per_lane: int = 0) -> int:
+    v = load().cellato_temporal_max_tile_rows(rule_id(rule), layout, word_bits, words_per_lane)
+    if v < 0:
+        check(-v)
+    return v
 
 
 def pack_cells(layout: int, word_bits: int, nb: int, cells_ptr: int, X: int, Y: int, planes, stream: int = 0) -> None:
@@ -185,21 +223,6 @@ def unpack_cells(layout: int, word_bits: int, nb: int, planes, X: int, Y: int, c
     check(load().cellato_unpack_cells(layout, word_bits, nb, ptr_array(planes), X, Y, cells_ptr, stream))
 
 
-def set_simple_variant(variant: int) -> None:
-    """0 automatic, 1 register-band kernel, 2 bulk-copy streaming kernel (linear layout)."""
-    check(load().cellato_set_simple_variant(variant))
-
-
-def set_temporal_variant(variant: int) -> None:
-    """0 automatic, 1 row-by-row reads, 2 hoisted reads per three-row trip (temporal kernel)."""
-    check(load().cellato_set_temporal_variant(variant))
-
-
-def set_temporal_width(words_per_lane: int) -> None:
-    """0 the rule's default, 1 or 2 words per lane of the temporal kernel."""
-    check(load().cellato_set_temporal_width(words_per_lane))
-
-
 def device_wait_timeouts() -> int:
     """Bounded device waits that gave up since the last call (0 when healthy)."""
     c = ctypes.c_uint(0)
@@ -210,10 +233,14 @@ def device_wait_timeouts() -> int:
 
 
 def run_temporal(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,
-                 k: int, tile_rows: int = 0, stream: int = 0) -> int:
+                 k: int, tile_rows: int = 0, stream: int = 0, row_loop: int = 0, words_per_lane: int = 0) -> int:
+    """k fused steps per launch; tile_rows, row_loop and words_per_lane as
+    cellato_tune (0 = the library's choice).  Returns 1 when the result ended
+    in planes_b, else 0."""
     out = ctypes.c_int(0)
+    t = tune(row_loop=row_loop, words_per_lane=words_per_lane, tile_rows=tile_rows)
     check(load().cellato_run_temporal(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),
-                                      X, Y, t0, steps, k, tile_rows, stream, ctypes.byref(out)))
+                                      X, Y, t0, steps, k, ctypes.byref(t), stream, ctypes.byref(out)))
     return out.value
 
 
@@ -275,3 +302,18 @@ def planes_to_bit_array(nb: int, layout: int, word_bits: int, planes, X: int, Y:
                         array_ptr: int, stream: int = 0) -> None:
     check(load().cellato_planes_to_bit_array(nb, layout, word_bits, ptr_array(planes), X, Y, array_word_bits,
                                              array_ptr, stream))
+
+
+def k_array(k_per_rule):
+    """A k-per-rule-id argument ({rule: k} or a sequence) as (ctypes int array
+    or None, entry count)."""
+    if k_per_rule is None:
+        return None, 0
+    if isinstance(k_per_rule, dict):
+        n = max((rule_id(r) for r in k_per_rule), default=-1) + 1
+        vals = [0] * n
+        for r, k in k_per_rule.items():
+            vals[rule_id(r)] = int(k)
+    else:
+        vals = [int(k) for k in k_per_rule]
+    return (ctypes.c_int * max(1, len(vals)))(*vals), len(vals)

@@ -31,9 +31,8 @@ class Server:
         cfg.layout, cfg.word_bits = layout, word_bits
         cfg.hbm_cap_bytes = hbm_cap_bytes
         cfg.tile_budget, cfg.chunk_rounds, cfg.max_inflight = tile_budget, chunk_rounds, max_inflight
-        ks = k_per_rule or {}
-        for r in range(10):
-            cfg.k_per_rule[r] = int(ks.get(r, 0) if isinstance(ks, dict) else ks[r])
+        self._ks, cfg.n_k_per_rule = lib.k_array(k_per_rule)  # the array outlives the create call
+        cfg.k_per_rule = self._ks
         h = ctypes.c_void_p()
         lib.check(L.cellato_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -24,7 +24,7 @@
 
 #include "capi_internal.hpp"
 #include "cellato_b200.h"
-#include "engine.cuh"
+#include "b200/engine.cuh"
 
 using namespace cellato::b200;
 using namespace cellato::b200::capi;

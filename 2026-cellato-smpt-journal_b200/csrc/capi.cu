@@ -3,9 +3,11 @@
 // engine.cuh and are instantiated per rule in rule_<automaton>.cu.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "cellato_b200.h"
@@ -36,11 +38,20 @@ int cuda_fail(cudaError_t e, const char* what) {
     return fail(CELLATO_ECUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
 }
 
+// The rule table: the ten built-in rules, then registered ones in order.
+// Entries are written once, before the count that publishes them, so readers
+// take no lock.
+namespace {
+const rule_ops* g_rules[CELLATO_MAX_RULES] = {&rule_ops_0, &rule_ops_1, &rule_ops_2, &rule_ops_3, &rule_ops_4,
+                                              &rule_ops_5, &rule_ops_6, &rule_ops_7, &rule_ops_8, &rule_ops_9};
+std::atomic<int> g_rule_count{CELLATO_BUILTIN_RULES};
+std::mutex g_register_mutex;
+}  // namespace
+
+int rule_count() { return g_rule_count.load(std::memory_order_acquire); }
+
 const rule_ops* ops_of(int rule) {
-    static const rule_ops* table[CELLATO_RULE_COUNT] = {&rule_ops_0, &rule_ops_1, &rule_ops_2, &rule_ops_3,
-                                                        &rule_ops_4, &rule_ops_5, &rule_ops_6, &rule_ops_7,
-                                                        &rule_ops_8, &rule_ops_9};
-    return (rule >= 0 && rule < CELLATO_RULE_COUNT) ? table[rule] : nullptr;
+    return (rule >= 0 && rule < rule_count()) ? g_rules[rule] : nullptr;
 }
 
 // Internal layout id and tile band height.
@@ -123,9 +134,39 @@ const char* cellato_last_error(void) { return g_last_error.c_str(); }
 int cellato_rule_from_name(const char* name) {
     if (!name) return -1;
     if (std::strcmp(name, "fire") == 0) return CELLATO_FOREST_FIRE;
-    for (int r = 0; r < CELLATO_RULE_COUNT; ++r)
+    const int n = rule_count();
+    for (int r = 0; r < n; ++r)
         if (std::strcmp(name, ops_of(r)->name) == 0) return r;
     return -1;
+}
+
+int cellato_rule_count(void) { return rule_count(); }
+
+int cellato_rule_register(const cellato_rule_ops* ops, int* rule_out) {
+    if (!ops || !rule_out) return fail(CELLATO_EINVAL, "ops and rule_out must not be NULL");
+    *rule_out = -1;
+    if (ops->abi_version != CELLATO_RULE_OPS_ABI || ops->struct_size != (int)sizeof(rule_ops))
+        return fail(CELLATO_EINVAL, "rule table built for rule_ops ABI %d (size %d); this library has ABI %d (size %d)",
+                    ops->abi_version, ops->struct_size, CELLATO_RULE_OPS_ABI, (int)sizeof(rule_ops));
+    if (!ops->name || !ops->name[0] || ops->planes < 1 || ops->planes > MAX_PLANES || ops->states < 1 ||
+        ops->states > 32 || !ops->simple || !ops->temporal || !ops->temporal_v || !ops->take_wait_timeouts ||
+        !ops->prepare_batch || !ops->temporal_batch || !ops->batch_blocks_per_sm)
+        return fail(CELLATO_EINVAL, "incomplete rule table");
+    std::lock_guard<std::mutex> lock(g_register_mutex);
+    const int n = rule_count();
+    for (int r = 0; r < n; ++r) {
+        if (g_rules[r] == ops) {
+            *rule_out = r;
+            return CELLATO_OK;
+        }
+        if (std::strcmp(g_rules[r]->name, ops->name) == 0 || std::strcmp(ops->name, "fire") == 0)
+            return fail(CELLATO_EINVAL, "a rule named \"%s\" is already registered", ops->name);
+    }
+    if (n >= CELLATO_MAX_RULES) return fail(CELLATO_EINVAL, "the rule table is full (%d rules)", CELLATO_MAX_RULES);
+    g_rules[n] = ops;
+    g_rule_count.store(n + 1, std::memory_order_release);
+    *rule_out = n;
+    return CELLATO_OK;
 }
 
 const char* cellato_rule_name(int rule) {
@@ -206,50 +247,46 @@ int cellato_planes_download(int nb, void* const* host_planes, const void* const*
     return CELLATO_OK;
 }
 
+static int check_tune(const cellato_tune* t) {
+    if (!t) return CELLATO_OK;
+    if (t->simple_kernel < 0 || t->simple_kernel > 2)
+        return fail(CELLATO_EINVAL, "tune.simple_kernel must be 0, 1 or 2 (got %d)", t->simple_kernel);
+    if (t->row_loop < 0 || t->row_loop > 2) return fail(CELLATO_EINVAL, "tune.row_loop must be 0, 1 or 2 (got %d)", t->row_loop);
+    if (t->words_per_lane < 0 || t->words_per_lane > 2)
+        return fail(CELLATO_EINVAL, "tune.words_per_lane must be 0, 1 or 2 (got %d)", t->words_per_lane);
+    if (t->tile_rows < 0) return fail(CELLATO_EINVAL, "tune.tile_rows must be >= 0 (got %d)", t->tile_rows);
+    return CELLATO_OK;
+}
+
 int cellato_run_simple(int rule, int layout, int word_bits, void* const* planes_a, void* const* planes_b,
-                       int x_cells, int y_cells, int t0, int steps, cellato_stream_t stream, int* result_in_b) {
+                       int x_cells, int y_cells, int t0, int steps, const cellato_tune* tune,
+                       cellato_stream_t stream, int* result_in_b) {
     const rule_ops* ops = ops_of(rule);
     if (!ops) return fail(CELLATO_EINVAL, "unknown rule id %d", rule);
     if (steps < 0) return fail(CELLATO_EINVAL, "steps must be >= 0 (got %d)", steps);
+    if (int rc = check_tune(tune)) return rc;
     if (int rc = check_dims(layout, word_bits, x_cells, y_cells)) return rc;
     plane_set a, b;
     if (int rc = make_sets(ops, planes_a, planes_b, a, b)) return rc;
     const int L = internal_layout(layout, word_bits);
     const int Xw = x_cells / 32;
+    const int variant = tune ? tune->simple_kernel : SIMPLE_AUTO;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     for (int i = 0; i < steps; ++i) {
         const plane_set& in = (i & 1) ? b : a;
         const plane_set& out = (i & 1) ? a : b;
-        cudaError_t e = ops->simple(L, in, out, Xw, y_cells, t0 + i, s);
+        cudaError_t e = ops->simple(L, in, out, Xw, y_cells, t0 + i, variant, s);
         if (e != cudaSuccess) return cuda_fail(e, "simple step launch");
     }
     if (result_in_b) *result_in_b = steps & 1;
     return CELLATO_OK;
 }
 
-int cellato_set_simple_variant(int variant) {
-    if (variant < 0 || variant > 2) return fail(CELLATO_EINVAL, "simple kernel variant must be 0, 1 or 2");
-    simple_variant() = variant;
-    return CELLATO_OK;
-}
-
-int cellato_set_temporal_width(int words_per_lane) {
-    if (words_per_lane < 0 || words_per_lane > 2)
-        return fail(CELLATO_EINVAL, "temporal words per lane must be 0, 1 or 2");
-    temporal_width() = words_per_lane;
-    return CELLATO_OK;
-}
-
-int cellato_set_temporal_variant(int variant) {
-    if (variant < 0 || variant > 2) return fail(CELLATO_EINVAL, "temporal kernel variant must be 0, 1 or 2");
-    temporal_variant() = variant;
-    return CELLATO_OK;
-}
-
 int cellato_device_wait_timeouts(unsigned* count) {
     if (!count) return fail(CELLATO_EINVAL, "count must not be NULL");
     *count = 0;
-    for (int r = 0; r < CELLATO_RULE_COUNT; ++r) {
+    const int n = rule_count();
+    for (int r = 0; r < n; ++r) {
         unsigned c = 0;
         cudaError_t e = ops_of(r)->take_wait_timeouts(&c);
         if (e != cudaSuccess) return cuda_fail(e, "reading the device wait-timeout counter");
@@ -258,30 +295,34 @@ int cellato_device_wait_timeouts(unsigned* count) {
     return *count ? fail(CELLATO_ETIMEDOUT, "%u bounded device waits gave up", *count) : CELLATO_OK;
 }
 
-int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits) {
+int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits, int words_per_lane) {
     const rule_ops* ops = ops_of(rule);
     if (!ops) return -fail(CELLATO_EINVAL, "unknown rule id %d", rule);
     if (word_bits != 32 && word_bits != 64) return -fail(CELLATO_EINVAL, "word_bits must be 32 or 64");
+    if (words_per_lane < 0 || words_per_lane > 2) return -fail(CELLATO_EINVAL, "words_per_lane must be 0, 1 or 2");
     const int R = band_height(layout, word_bits);
-    const int row_bytes = ops->planes * 32 * ops->temporal_v_now() * 4;
+    const int row_bytes = ops->planes * 32 * ops->temporal_v(words_per_lane) * 4;
     const int q = std::max(ops->temporal_warps, R);
     return (max_optin_smem() / row_bytes) / q * q;
 }
 
 int cellato_run_temporal(int rule, int layout, int word_bits, void* const* planes_a, void* const* planes_b,
-                         int x_cells, int y_cells, int t0, int steps, int k, int tile_rows, cellato_stream_t stream,
-                         int* result_in_b) {
+                         int x_cells, int y_cells, int t0, int steps, int k, const cellato_tune* tune,
+                         cellato_stream_t stream, int* result_in_b) {
     const rule_ops* ops = ops_of(rule);
     if (!ops) return fail(CELLATO_EINVAL, "unknown rule id %d", rule);
     if (steps < 0) return fail(CELLATO_EINVAL, "steps must be >= 0 (got %d)", steps);
     if (k < 1 || k > 32) return fail(CELLATO_EINVAL, "temporal_steps must be in 1..32 (got %d)", k);
+    if (int rc = check_tune(tune)) return rc;
     if (int rc = check_dims(layout, word_bits, x_cells, y_cells)) return rc;
     plane_set a, b;
     if (int rc = make_sets(ops, planes_a, planes_b, a, b)) return rc;
     const int L = internal_layout(layout, word_bits);
     const int R = band_height(layout, word_bits);
     const int q = std::max(ops->temporal_warps, R);
-    const int V = ops->temporal_v_now();
+    const int V = ops->temporal_v(tune ? tune->words_per_lane : 0);
+    const int loop = tune ? tune->row_loop : LOOP_AUTO;
+    const int tile_rows = tune ? tune->tile_rows : 0;
     const int TH = tile_rows > 0 ? tile_rows : default_tile_rows(ops, R, k, V, ops->planes == 1 ? 128 : 224);
     if (TH % q != 0)
         return fail(CELLATO_EINVAL, "temporal tile rows %d must be a multiple of %d", TH, q);
@@ -298,7 +339,7 @@ int cellato_run_temporal(int rule, int layout, int word_bits, void* const* plane
             return fail(CELLATO_EINVAL, "temporal tile of %d rows leaves no interior for %d steps", TH, kk);
         const plane_set& in = (launches & 1) ? b : a;
         const plane_set& out = (launches & 1) ? a : b;
-        cudaError_t e = ops->temporal(L, in, out, Xw, y_cells, t0 + done, kk, TH, HY, s);
+        cudaError_t e = ops->temporal(L, in, out, Xw, y_cells, t0 + done, kk, TH, HY, loop, V, s);
         if (e != cudaSuccess) return cuda_fail(e, "temporal launch");
         done += kk;
         ++launches;

@@ -7,12 +7,13 @@
 
 #include <cstdint>
 
-#include "rule_kernels.cuh"
+#include "b200/rule_kernels.cuh"
 
 namespace cellato::b200::capi {
 int fail(int status, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
 const rule_ops* ops_of(int rule);
+int rule_count();  // rule ids in use (built-in + registered)
 int internal_layout(int layout, int word_bits);
 int band_height(int layout, int word_bits);
 int check_dims(int layout, int word_bits, int X, int Y);

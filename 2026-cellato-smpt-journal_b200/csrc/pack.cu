@@ -15,7 +15,7 @@
 #include <cstdint>
 
 #include "cellato_b200.h"
-#include "engine.cuh"
+#include "b200/engine.cuh"
 
 using namespace cellato::b200;
 

@@ -1,5 +1,5 @@
 // Kernels of the critters automaton (rule id 8).
-#include "rule_kernels.cuh"
+#include "b200/rule_kernels.cuh"
 #include "critters/config.hpp"
 
 CELLATO_DEFINE_RULE_OPS(8, critters::config)

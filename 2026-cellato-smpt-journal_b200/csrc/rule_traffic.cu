@@ -1,5 +1,5 @@
 // Kernels of the traffic automaton (rule id 9).
-#include "rule_kernels.cuh"
+#include "b200/rule_kernels.cuh"
 #include "traffic/config.hpp"
 
 CELLATO_DEFINE_RULE_OPS(9, traffic::config)

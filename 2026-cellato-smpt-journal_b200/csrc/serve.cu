@@ -76,11 +76,13 @@ struct cellato_server_st {
     sv::scheduler sched{sv::limits{}};
     cudaMemPool_t pool = nullptr;
     cudaStream_t main_stream = nullptr;
-    cudaStream_t rs[CELLATO_RULE_COUNT] = {};
     cudaEvent_t fork = nullptr;
-    cudaEvent_t join[CELLATO_RULE_COUNT] = {};
-    int TH[CELLATO_RULE_COUNT] = {}, HY[CELLATO_RULE_COUNT] = {};
-    int per_sm[CELLATO_RULE_COUNT] = {};  // resident CTAs per SM of each rule's batched kernel
+    // per rule id, set up when the first request of that rule is submitted
+    // (rules registered after the server was created work too)
+    std::vector<cudaStream_t> rs;
+    std::vector<cudaEvent_t> join;
+    std::vector<int> TH, HY;
+    std::vector<int> per_sm;  // resident CTAs per SM of each rule's batched kernel (0: not set up)
     std::vector<slot> slots;
     int next_slot = 0;
     std::deque<inflight_rec> inflight;
@@ -113,7 +115,7 @@ void destroy_all(cellato_server_st* s) {
         if (sl.done) cudaEventDestroy(sl.done);
     }
     if (m) cudaStreamSynchronize(m);
-    for (int r = 0; r < CELLATO_RULE_COUNT; ++r) {
+    for (size_t r = 0; r < s->rs.size(); ++r) {
         if (s->rs[r]) cudaStreamDestroy(s->rs[r]);
         if (s->join[r]) cudaEventDestroy(s->join[r]);
     }
@@ -223,6 +225,31 @@ int materialise(cellato_server_st* s, long long id) {
     return CELLATO_OK;
 }
 
+// Tile shape, kernel attributes, stream and join event of a rule, on the
+// first request of it.
+int ensure_rule(cellato_server_st* s, int rule) {
+    if ((int)s->per_sm.size() > rule && s->per_sm[rule] > 0) return CELLATO_OK;
+    const rule_ops* ops = ops_of(rule);
+    if ((int)s->per_sm.size() <= rule) {
+        s->rs.resize(rule + 1, nullptr);
+        s->join.resize(rule + 1, nullptr);
+        s->TH.resize(rule + 1, 0);
+        s->HY.resize(rule + 1, 0);
+        s->per_sm.resize(rule + 1, 0);
+    }
+    const int k = s->sched.lim().k_of(rule);
+    s->TH[rule] = default_tile_rows(ops, s->R, k, ops->batch_words_per_lane);
+    s->HY[rule] = (k + s->R - 1) / s->R * s->R;
+    if (s->TH[rule] - 2 * s->HY[rule] <= 0)
+        return fail(CELLATO_EINVAL, "rule %d: a %d-row tile leaves no interior for k=%d", rule, s->TH[rule], k);
+    cudaError_t e = ops->prepare_batch(s->internal, s->TH[rule]);
+    if (e == cudaSuccess && !s->rs[rule]) e = cudaStreamCreateWithFlags(&s->rs[rule], cudaStreamNonBlocking);
+    if (e == cudaSuccess && !s->join[rule]) e = cudaEventCreateWithFlags(&s->join[rule], cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "setting up a rule's batched kernel");
+    s->per_sm[rule] = ops->batch_blocks_per_sm(s->internal, s->TH[rule]);
+    return CELLATO_OK;
+}
+
 int submit_common(cellato_server_t s, int rule, int x, int y, int steps, int t0, int keep, req_rec& r,
                   long long* id) {
     if (!s || !id) return fail(CELLATO_EINVAL, "server and id must not be NULL");
@@ -231,6 +258,7 @@ int submit_common(cellato_server_t s, int rule, int x, int y, int steps, int t0,
     if (!ops) return fail(CELLATO_EINVAL, "unknown rule id %d", rule);
     if (steps < 0) return fail(CELLATO_EINVAL, "negative step count");
     if (int rc = check_dims(s->layout, s->word_bits, x, y)) return rc;
+    if (int rc = ensure_rule(s, rule)) return rc;
     r.rule = rule, r.x = x, r.y = y, r.steps = steps, r.nb = ops->planes;
     r.keep = keep != 0;
     r.t0 = t0;
@@ -253,10 +281,12 @@ int cellato_server_create(const cellato_server_config* cfg, cellato_server_t* ou
     *out = nullptr;
     if (int rc = check_dims(cfg->layout, cfg->word_bits, 64, 64)) return rc;
     sv::limits lim;
-    for (int r = 0; r < CELLATO_RULE_COUNT; ++r) {
+    if (cfg->n_k_per_rule < 0 || (cfg->n_k_per_rule > 0 && !cfg->k_per_rule))
+        return fail(CELLATO_EINVAL, "bad k_per_rule array");
+    for (int r = 0; r < cfg->n_k_per_rule; ++r) {
         const int k = cfg->k_per_rule[r];
         if (k < 0 || k > 32) return fail(CELLATO_EINVAL, "k for rule %d must be in 1..32 (0 = 16), got %d", r, k);
-        lim.k[r] = k ? k : 16;
+        lim.k.push_back(k ? k : 16);
     }
     auto* s = new cellato_server_st;
     s->layout = cfg->layout;
@@ -277,20 +307,6 @@ int cellato_server_create(const cellato_server_config* cfg, cellato_server_t* ou
     // three CTAs per SM, enough to fill the device with each automaton's launch
     lim.tile_budget = cfg->tile_budget > 0 ? cfg->tile_budget : 32LL * s->sms;
     lim.chunk_rounds = cfg->chunk_rounds > 0 ? cfg->chunk_rounds : 4;
-    for (int r = 0; r < CELLATO_RULE_COUNT; ++r) {
-        const rule_ops* ops = ops_of(r);
-        s->TH[r] = default_tile_rows(ops, s->R, lim.k[r], ops->batch_words_per_lane);
-        s->HY[r] = (lim.k[r] + s->R - 1) / s->R * s->R;
-        if (s->TH[r] - 2 * s->HY[r] <= 0) {
-            destroy_all(s);
-            return fail(CELLATO_EINVAL, "rule %d: a %d-row tile leaves no interior for k=%d", r, s->TH[r], lim.k[r]);
-        }
-        if ((e = ops->prepare_batch(s->internal, s->TH[r])) != cudaSuccess) {
-            destroy_all(s);
-            return cuda_fail(e, "batch kernel attributes");
-        }
-        s->per_sm[r] = ops->batch_blocks_per_sm(s->internal, s->TH[r]);
-    }
     s->sched = sv::scheduler(lim);
 
     cudaMemPoolProps props{};
@@ -304,10 +320,6 @@ int cellato_server_create(const cellato_server_config* cfg, cellato_server_t* ou
     }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->main_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming);
-    for (int r = 0; r < CELLATO_RULE_COUNT && e == cudaSuccess; ++r) {
-        e = cudaStreamCreateWithFlags(&s->rs[r], cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->join[r], cudaEventDisableTiming);
-    }
     s->slots.resize(s->max_inflight);
     for (auto& sl : s->slots)
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
@@ -378,18 +390,24 @@ int cellato_server_iterate(cellato_server_t s, int* active) {
         return rc < 0 ? -rc : CELLATO_OK;
     }
 
-    // work list: one descriptor per active request, then every round's items
+    // work list: one descriptor per active request, then per automaton the items
+    // of all its rounds (ordered by round); each automaton's rounds are one
+    // persistent launch in which a request's next round starts when its
+    // previous one is done
     std::unordered_map<long long, int> desc_of;
     std::vector<batch_grid_desc> descs;
     descs.reserve(plan.active.size());
     for (long long id : plan.active) {
         const req_rec& r = s->recs[id];
+        const rule_ops* ops = ops_of(r.rule);
+        const int effW = 32 * ops->batch_words_per_lane - 2, effH = s->TH[r.rule] - 2 * s->HY[r.rule];
         desc_of[id] = (int)descs.size();
         batch_grid_desc d{};
         d.p[0] = r.p[0];
         d.p[1] = r.p[1];
         d.Xw = r.x / 32;
         d.Y = r.y;
+        d.tiles = ((d.Xw + effW - 1) / effW) * ((r.y + effH - 1) / effH);
         descs.push_back(d);
     }
     struct launch_rec {
@@ -397,52 +415,60 @@ int cellato_server_iterate(cellato_server_t s, int* active) {
     };
     std::vector<batch_item> items;
     std::vector<launch_rec> launches;
-    for (int rule = 0; rule < CELLATO_RULE_COUNT; ++rule) {
+    for (int rule = 0; rule < (int)plan.rounds.size(); ++rule) {
+        if (plan.rounds[rule].empty()) continue;
         const rule_ops* ops = ops_of(rule);
         const int effW = 32 * ops->batch_words_per_lane - 2, effH = s->TH[rule] - 2 * s->HY[rule];
-        for (const auto& round : plan.rounds[rule]) {
-            const int first = (int)items.size();
-            for (const sv::round_entry& en : round) {
+        const int first = (int)items.size();
+        for (size_t q = 0; q < plan.rounds[rule].size(); ++q) {
+            for (const sv::round_entry& en : plan.rounds[rule][q]) {
                 const req_rec& r = s->recs[en.id];
                 const int tx = (r.x / 32 + effW - 1) / effW, ty = (r.y + effH - 1) / effH;
-                const int flags = en.steps | (en.src ? BATCH_FLIP_BUFFER : 0) | (en.tpar ? BATCH_FLIP_TIME : 0);
+                const int flags = en.steps | (en.src ? BATCH_FLIP_BUFFER : 0) | (en.tpar ? BATCH_FLIP_TIME : 0) |
+                                  ((int)q << BATCH_ROUND_SHIFT);
                 const int g = desc_of[en.id];
                 for (int yy = 0; yy < ty; ++yy)
                     for (int xx = 0; xx < tx; ++xx) items.push_back(batch_item{g, xx, yy, flags});
             }
-            launches.push_back(launch_rec{rule, first, (int)items.size() - first});
         }
+        launches.push_back(launch_rec{rule, first, (int)items.size() - first});
     }
     const size_t desc_bytes = round_up(descs.size() * sizeof(batch_grid_desc), ALIGN);
     const size_t item_bytes = round_up(items.size() * sizeof(batch_item), ALIGN);
+    // queue head per launch, finished-tile count per descriptor; cleared each iteration
+    const size_t sync_words = launches.size() + descs.size();
+    const size_t sync_bytes = round_up(sync_words * sizeof(unsigned), ALIGN);
     const size_t sums_bytes = plan.finishing.size() * 16 * sizeof(unsigned long long);
     const int si = s->next_slot;
     slot& sl = s->slots[si];
-    if (int rc = ensure_slot(s, sl, desc_bytes + item_bytes + sums_bytes + ALIGN)) return rc;
+    if (int rc = ensure_slot(s, sl, desc_bytes + item_bytes + sync_bytes + sums_bytes + ALIGN)) return rc;
     std::memcpy(sl.host, descs.data(), descs.size() * sizeof(batch_grid_desc));
     std::memcpy(sl.host + desc_bytes, items.data(), items.size() * sizeof(batch_item));
+    std::memset(sl.host + desc_bytes + item_bytes, 0, sync_bytes);
     cudaStream_t m = s->main_stream;
-    cudaError_t e = cudaMemcpyAsync(sl.dev, sl.host, desc_bytes + item_bytes, cudaMemcpyHostToDevice, m);
+    cudaError_t e = cudaMemcpyAsync(sl.dev, sl.host, desc_bytes + item_bytes + sync_bytes, cudaMemcpyHostToDevice, m);
     if (e != cudaSuccess) return server_cuda_fail(s, e, "cudaMemcpyAsync (server work list)");
     const auto* d_descs = reinterpret_cast<const batch_grid_desc*>(sl.dev);
     const auto* d_items = reinterpret_cast<const batch_item*>(sl.dev + desc_bytes);
+    auto* d_sync = reinterpret_cast<unsigned*>(sl.dev + desc_bytes + item_bytes);
+    unsigned* d_done = d_sync + launches.size();
 
     if ((e = cudaEventRecord(s->fork, m)) != cudaSuccess) return server_cuda_fail(s, e, "cudaEventRecord");
-    bool used[CELLATO_RULE_COUNT] = {};
-    for (const launch_rec& L : launches) {
+    std::vector<char> used(s->rs.size(), 0);
+    for (size_t li = 0; li < launches.size(); ++li) {
+        const launch_rec& L = launches[li];
         if (L.count == 0) continue;
         cudaStream_t st = s->rs[L.rule];
-        if (!used[L.rule]) {
-            used[L.rule] = true;
-            if ((e = cudaStreamWaitEvent(st, s->fork, 0)) != cudaSuccess)
-                return server_cuda_fail(s, e, "cudaStreamWaitEvent");
-        }
+        used[L.rule] = 1;
+        if ((e = cudaStreamWaitEvent(st, s->fork, 0)) != cudaSuccess)
+            return server_cuda_fail(s, e, "cudaStreamWaitEvent");
         e = ops_of(L.rule)->temporal_batch(s->internal, d_descs, d_items + L.first, L.count, 0, 0, s->TH[L.rule],
-                                           s->HY[L.rule], std::min(L.count, s->per_sm[L.rule] * s->sms), st);
+                                           s->HY[L.rule], d_sync + li, d_done,
+                                           std::min(L.count, s->per_sm[L.rule] * s->sms), st);
         if (e != cudaSuccess) return server_cuda_fail(s, e, "batched temporal launch (server)");
         ++s->launches;
     }
-    for (int rule = 0; rule < CELLATO_RULE_COUNT; ++rule) {
+    for (int rule = 0; rule < (int)used.size(); ++rule) {
         if (!used[rule]) continue;
         if ((e = cudaEventRecord(s->join[rule], s->rs[rule])) != cudaSuccess ||
             (e = cudaStreamWaitEvent(m, s->join[rule], 0)) != cudaSuccess)
@@ -452,7 +478,7 @@ int cellato_server_iterate(cellato_server_t s, int* active) {
     // finishing requests: checksums on the device, one copy back, free unkept planes
     inflight_rec f;
     f.slot = si;
-    f.sums_off = desc_bytes + item_bytes;
+    f.sums_off = desc_bytes + item_bytes + sync_bytes;
     f.finishing = plan.finishing;
     auto* d_sums = reinterpret_cast<unsigned long long*>(sl.dev + f.sums_off);
     for (size_t j = 0; j < plan.finishing.size(); ++j) {

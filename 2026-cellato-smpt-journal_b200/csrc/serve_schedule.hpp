@@ -16,10 +16,11 @@
 // Each iteration activates resident requests in admission order, first fit,
 // while the sum of their tiles stays within the budget (the oldest one always
 // runs), and advances each active request by up to chunk_rounds rounds of k
-// steps (k per automaton).  Round r of an iteration is one batched launch per
-// automaton over the tiles of every active request that has an r-th round.
-// Each request's rounds carry its own step parity and ping-pong buffer, so
-// requests admitted at different times share launches.
+// steps (k per automaton).  Round r of an iteration covers the tiles of every
+// active request of an automaton that has an r-th round; the device runs all
+// rounds of one automaton in one persistent launch.  Each request's rounds
+// carry its own step parity and ping-pong buffer, so requests admitted at
+// different times share launches.
 #ifndef CELLATO_B200_SERVE_SCHEDULE_HPP
 #define CELLATO_B200_SERVE_SCHEDULE_HPP
 
@@ -30,8 +31,6 @@
 #include <vector>
 
 namespace cellato::b200::serve {
-
-constexpr int RULES = 10;
 
 enum class phase : int { waiting = 0, resident = 1, finished = 2 };
 
@@ -63,7 +62,7 @@ struct finish_entry {
 };
 
 struct iteration_plan {
-    std::vector<std::vector<round_entry>> rounds[RULES];  // rounds[rule][r]
+    std::vector<std::vector<std::vector<round_entry>>> rounds;  // rounds[rule][r] (rules seen so far)
     std::vector<long long> active;                        // requests advanced (admission order)
     std::vector<finish_entry> finishing;
     long long cell_steps = 0;
@@ -75,7 +74,11 @@ struct limits {
     long long cap_bytes = 0;    // resident bytes allowed
     long long tile_budget = 1;  // tiles per round over all active requests
     int chunk_rounds = 4;       // rounds per request per iteration
-    int k[RULES] = {16, 16, 16, 16, 16, 16, 16, 16, 16, 16};
+    std::vector<int> k;         // steps per round by rule id; missing or 0 entries: 16
+    int k_of(int rule) const {
+        const int v = rule >= 0 && rule < (int)k.size() ? k[rule] : 0;
+        return std::max(1, std::min(v > 0 ? v : 16, 32));
+    }
 };
 
 class scheduler {
@@ -122,7 +125,7 @@ public:
         for (long long id : order_) {
             request& r = reqs_[id];
             const int left = r.steps - r.done;
-            const int k = std::max(1, std::min(lim_.k[r.rule], 32));
+            const int k = lim_.k_of(r.rule);
             const int chunk = std::min(left, lim_.chunk_rounds * k);
             const long long t = chunk > 0 ? r.tiles : 0;
             if (!p.active.empty() && used + t > lim_.tile_budget) {
@@ -131,6 +134,7 @@ public:
             }
             used += t;
             p.active.push_back(id);
+            if ((int)p.rounds.size() <= r.rule) p.rounds.resize(r.rule + 1);
             auto& rr = p.rounds[r.rule];
             for (int s = 0, q = 0; s < chunk; s += k, ++q) {
                 const int n = std::min(k, chunk - s);

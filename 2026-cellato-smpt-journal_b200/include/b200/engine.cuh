@@ -66,24 +66,38 @@ __device__ __forceinline__ void transpose4x4(word& a, word& b, word& c, word& d)
     d = __byte_perm(v, x, 0x7632);             // a3 b3 c3 d3
 }
 
+// Global loads of plane words.  Kernels whose input is not written while they
+// run read through the read-only data cache (ld.global.nc); the persistent
+// batched kernel, whose later rounds read what its earlier rounds wrote in the
+// same launch, reads at L2 (ld.global.cg), which no stale L1 line can shadow.
+enum : int { LOAD_NC = 0, LOAD_CG = 1 };
+
+template <int LOAD, class T>
+__device__ __forceinline__ T gload(const T* p) {
+    if constexpr (LOAD == LOAD_CG)
+        return __ldcg(p);
+    else
+        return __ldg(p);
+}
+
 // Load the R rows of linear word gx of band b (tile row b) of one plane.
 //   linear: R == 1, word gx of row b.
 //   tiled : tiles 4gx .. 4gx+3 of tile row b, transposed to R row words.
-template <int LAYOUT>
+template <int LAYOUT, int LOAD = LOAD_NC>
 __device__ __forceinline__ void load_word_rows(const word* __restrict__ plane, int Xw, int b, int gx,
                                                word (&rows)[band_rows<LAYOUT>()]) {
     if constexpr (LAYOUT == LAYOUT_LINEAR) {
-        rows[0] = __ldg(plane + (size_t)b * Xw + gx);
+        rows[0] = gload<LOAD>(plane + (size_t)b * Xw + gx);
     } else if constexpr (LAYOUT == LAYOUT_TILED4) {
         // 4 tiles x 4 bytes = one 16-byte vector
-        const uint4 t = __ldg(reinterpret_cast<const uint4*>(plane + ((size_t)b * Xw + gx) * 4));
+        const uint4 t = gload<LOAD>(reinterpret_cast<const uint4*>(plane + ((size_t)b * Xw + gx) * 4));
         word a = t.x, bb = t.y, c = t.z, d = t.w;
         transpose4x4(a, bb, c, d);
         rows[0] = a, rows[1] = bb, rows[2] = c, rows[3] = d;
     } else {
         // 4 tiles x 8 bytes: (lo, hi) per tile; lo = rows 0-3, hi = rows 4-7
         const uint4* src = reinterpret_cast<const uint4*>(plane + ((size_t)b * Xw + gx) * 8);
-        const uint4 t01 = __ldg(src), t23 = __ldg(src + 1);
+        const uint4 t01 = gload<LOAD>(src), t23 = gload<LOAD>(src + 1);
         word l0 = t01.x, l1 = t01.z, l2 = t23.x, l3 = t23.z;
         word h0 = t01.y, h1 = t01.w, h2 = t23.y, h3 = t23.w;
         transpose4x4(l0, l1, l2, l3);
@@ -422,10 +436,13 @@ __global__ void __launch_bounds__(WARPS * 32) simple_step_kernel(plane_set in, p
 // word, where the first idle lane reads it.  Needs Xw % 4 == 0 (16-byte rows).
 //
 // Every mbarrier wait is bounded: a wait that gives up records the failure in
-// g_stream_wait_timeouts, drains the copies this warp still has in flight
-// (again bounded) and returns; the host reads and clears the counter through
-// the rule's status entry.
-static __device__ unsigned g_stream_wait_timeouts = 0;
+// g_wait_timeouts, drains the copies this warp still has in flight (again
+// bounded) and returns; the host reads and clears the counter through the
+// rule's status entry.
+//
+// g_wait_timeouts counts every bounded device-side wait of one rule's kernels
+// that gave up (one counter per translation unit, i.e. per rule).
+static __device__ unsigned g_wait_timeouts = 0;
 
 constexpr int STREAM_STAGES = 3;
 constexpr int STREAM_BAND = 4;
@@ -587,10 +604,11 @@ __global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, p
         }
     }
     if (failed_at >= 0) {
-        if (lane == 0) atomicAdd(&g_stream_wait_timeouts, 1u);
+        if (lane == 0) atomicAdd(&g_wait_timeouts, 1u);
         // drain the copies this warp still has in flight (chunks failed_at ..
-        // failed_at + S - 1 were issued) before the CTA's shared memory is released
-        for (int c = failed_at + 1; c < min(nchunks, failed_at + S); ++c)
+        // failed_at + S - 1 were issued, the one that timed out included) before
+        // the CTA's shared memory is released
+        for (int c = failed_at; c < min(nchunks, failed_at + S); ++c)
             mbar_wait_bounded(&bars[c % S], (unsigned)(c / S) & 1u);
     }
 }
@@ -616,7 +634,9 @@ __global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, p
 // trip before the trip's writes; false reads each row just before the row
 // above it is evaluated.  Both compute the same values; which is faster
 // depends on the rule's register use and the occupancy (the autotuner picks).
-template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST = true>
+// LOAD: how the tile is read from global memory (LOAD_NC, or LOAD_CG when the
+// input may have been written earlier in the same launch).
+template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST = true, int LOAD = LOAD_NC>
 __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                                               int TH, int HY, int bx, int by) {
     constexpr int R = band_rows<LAYOUT>();
@@ -647,7 +667,7 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
 #pragma unroll
             for (int p = 0; p < NB; ++p) {
                 word rows[R];
-                load_word_rows<LAYOUT>(in.p[p], Xw, bw, gx, rows);
+                load_word_rows<LAYOUT, LOAD>(in.p[p], Xw, bw, gx, rows);
 #pragma unroll
                 for (int r = 0; r < R; ++r) at(p, band * R + r, s) = rows[r];
             }
@@ -844,41 +864,87 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plan
 }
 
 // ======================================================= batched temporal kernel
-// Many independent grids of one rule in one launch: persistent CTAs stride over
-// a device work list of (grid, tile, steps) items and run the temporal tile of
-// each item.  Every grid has its own planes (p[0] = a, p[1] = b), sizes and
-// step budget; all items use the launch's halo HY, which covers their step
-// count (steps <= k).  By default all items read p[parity] and start at the
-// launch's global step t0.  Two flag bits above the step count let items of one
-// launch sit at different points of their runs (a server advancing requests
-// admitted at different times): BATCH_FLIP_BUFFER reads p[parity ^ 1] instead,
-// BATCH_FLIP_TIME starts at t0 + 1.  Only the parity of a step number matters
-// to the rules (alternation and Margolus phase), so one bit covers any start.
+// Many independent grids of one rule, every round of every grid, in ONE
+// persistent launch.  The work list holds an item per (grid, round, tile),
+// ordered by round.  Resident CTAs claim items in list order from a device
+// queue head; a grid's round r may start once all its tiles of round r - 1 are
+// done, which each item checks against the grid's count of finished tiles:
+//   * round r reads the buffer round r - 1 wrote (read after write), and
+//   * writes the buffer round r - 1 read (write after read),
+// so "every tile of round r - 1 finished" orders both.  A CTA only ever waits
+// for items earlier in the list, which CTAs that are running have claimed, so
+// the waits cannot deadlock whatever the number of resident CTAs.  Every wait
+// is bounded; one that gives up counts in g_wait_timeouts and the item runs
+// anyway, so the launch always ends.
+//
+// Each grid has its own planes (p[0] = a, p[1] = b), sizes and tile count.
+// Items carry in their `steps` word: the step count (low 8 bits, at most the
+// launch's halo HY), BATCH_FLIP_BUFFER (read p[parity ^ 1]), BATCH_FLIP_TIME
+// (the first step number is t0 + 1; only the parity of a step number matters
+// to the rules), and the item's round within the launch (bits 10 and up).
 struct batch_grid_desc {
     plane_set p[2];
     int Xw, Y;
+    int tiles;  // tiles of one round of this grid
+    int pad_;
 };
 
 struct batch_item {
-    int grid, tx, ty, steps;  // steps: count in the low 8 bits, then the flags
+    int grid, tx, ty, steps;  // steps: count, flags and round (see above)
 };
 
 constexpr int BATCH_STEPS_MASK = 0xff;
 constexpr int BATCH_FLIP_BUFFER = 1 << 8;
 constexpr int BATCH_FLIP_TIME = 1 << 9;
+constexpr int BATCH_ROUND_SHIFT = 10;
+constexpr unsigned BATCH_WAIT_LIMIT = 1u << 24;  // polls of 64 ns sleeps: about a second
 
+__device__ __forceinline__ unsigned load_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// head: the launch's queue head; done[g]: finished tiles of grid g.  Both start
+// at zero (the host clears them before the launch).
 template <class Net, int NB, int LAYOUT, int V, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) temporal_batch_kernel(const batch_grid_desc* __restrict__ grids,
                                                                     const batch_item* __restrict__ items, int n_items,
-                                                                    int parity, int t0, int TH, int HY) {
-    for (int i = blockIdx.x; i < n_items; i += gridDim.x) {
+                                                                    int parity, int t0, int TH, int HY,
+                                                                    unsigned* head, unsigned* done) {
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(head, 1u);
+        __syncthreads();
+        const int i = s_item;
+        if (i >= n_items) break;
         const batch_item it = items[i];
         const batch_grid_desc& g = grids[it.grid];
+        const unsigned round = (unsigned)it.steps >> BATCH_ROUND_SHIFT;
+        if (round > 0 && threadIdx.x == 0) {
+            const unsigned need = round * (unsigned)g.tiles;
+            unsigned polls = 0;
+            while (load_acquire_gpu(done + it.grid) < need) {
+                if (++polls == BATCH_WAIT_LIMIT) {
+                    atomicAdd(&g_wait_timeouts, 1u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __syncthreads();
         const int src = parity ^ ((it.steps & BATCH_FLIP_BUFFER) ? 1 : 0);
         const int start = t0 + ((it.steps & BATCH_FLIP_TIME) ? 1 : 0);
-        temporal_tile<Net, NB, LAYOUT, V, WARPS>(g.p[src], g.p[src ^ 1], g.Xw, g.Y, start, it.steps & BATCH_STEPS_MASK,
-                                                  TH, HY, it.tx, it.ty);
-        __syncthreads();  // the next item reloads the tile
+        temporal_tile<Net, NB, LAYOUT, V, WARPS, true, LOAD_CG>(g.p[src], g.p[src ^ 1], g.Xw, g.Y, start,
+                                                               it.steps & BATCH_STEPS_MASK, TH, HY, it.tx, it.ty);
+        // publish the tile: every thread's stores are visible device-wide
+        // before the count that releases the next round
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(done + it.grid, 1u);
+        }
     }
 }
 

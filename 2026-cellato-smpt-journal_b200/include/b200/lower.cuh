@@ -710,7 +710,8 @@ struct lower<Dict, Targets,
             const count_cache& m = c.mid.cc[slot];
             return a.P[0] | a.P[1] | a.P[2] | b.P[0] | b.P[1] | b.P[2] | m.P[0] | m.P[2];
         } else {
-            return gt(lower<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>>::eval(c),
+            // through ev, so that a symbolic context substitutes the count signal
+            return gt(ev<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>>(c),
                       from_constant<(long long)Z>());
         }
     }
@@ -726,8 +727,7 @@ struct lower<Dict, Targets,
         if constexpr (Z == 0) {
             return c.up.cc[slot].P[1] | c.dn.cc[slot].P[1] | c.mid.cc[slot].P[0] | c.mid.cc[slot].P[2];
         } else {
-            return gt(lower<Dict, Targets,
-                            ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>>::eval(c),
+            return gt(ev<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>>(c),
                       from_constant<(long long)Z>());
         }
     }

@@ -1,9 +1,18 @@
 // Per-rule launchers: instantiate the engine kernels for one automaton config
-// and expose them through a rule_ops table (one table per rule, one .cu file
-// per rule so the ten rules compile in parallel).  This is the B200
-// counterpart of the reference's explicit instantiations
+// and expose them through a rule_ops table.  This is the B200 counterpart of
+// the reference's explicit instantiations
 // (src/_shared/cuda_instantiation_template.cuh:77-193): the rule stays a C++
-// type and is lowered at compile time; the C ABI selects it by id.
+// type and is lowered at compile time; the C ABI selects it by rule id.
+//
+// The ten automata of the reference are instantiated inside the library (one
+// .cu file per rule, so they compile in parallel).  Any other rule written in
+// the same DSL is instantiated by the caller's own translation unit, compiled
+// with nvcc for sm_100a: cellato::b200::custom_rule_ops<Config>() builds its
+// table there and cellato_rule_register hands it to the library, which then
+// runs it under a new rule id through every entry point (b200/custom_rule.cuh).
+//
+// Nothing here holds mutable state: which kernel variant, row loop and tile
+// width a launch uses are arguments of each call (cellato_tune in the C ABI).
 #ifndef CELLATO_B200_RULE_KERNELS_CUH
 #define CELLATO_B200_RULE_KERNELS_CUH
 
@@ -11,59 +20,57 @@
 
 #include <algorithm>
 
-#include "engine.cuh"
+#include "b200/engine.cuh"
+
+// Version of the rule_ops layout; cellato_rule_register refuses a table built
+// against another version.
+#define CELLATO_RULE_OPS_ABI 3
 
 namespace cellato::b200 {
+// Single-step kernel choices (cellato_tune::simple_kernel).
+enum : int { SIMPLE_AUTO = 0, SIMPLE_REGISTER = 1, SIMPLE_STREAM = 2 };
+// Temporal row loops (cellato_tune::row_loop).
+enum : int { LOOP_AUTO = 0, LOOP_ROW_BY_ROW = 1, LOOP_HOISTED = 2 };
+}  // namespace cellato::b200
 
-// Single-step kernel for the linear layout: 0 = the library's choice, 1 = the
-// register-band kernel, 2 = the bulk-copy streaming kernel.  Process-wide.
-inline int& simple_variant() {
-    static int v = 0;
-    return v;
-}
-
-// Row loop of the temporal kernel: 0 = the library's choice (hoisted reads),
-// 1 = row by row, 2 = hoisted reads of each 3-row trip.  Process-wide.
-inline int& temporal_variant() {
-    static int v = 0;
-    return v;
-}
-
-// Words per lane of the single-grid temporal kernel: 0 = the library's default
-// (two for one-plane rules, else one), 1 = one word per lane (half the
-// registers and shared memory per row, so more CTAs per SM), 2 = two (rules of
-// up to three planes only; others use one).  Process-wide.
-inline int& temporal_width() {
-    static int v = 0;
-    return v;
-}
-
-struct rule_ops {
+// The kernels of one rule, as function pointers into the translation unit that
+// instantiated them.  Plain data, built once per rule and never modified.
+struct cellato_rule_ops_st {
+    int abi_version;  // CELLATO_RULE_OPS_ABI
+    int struct_size;  // sizeof(cellato_rule_ops_st)
     const char* name;
     int planes;  // needed_bits
     int states;  // number_of_values
-    // one time step t (its parity selects the instantiation)
-    cudaError_t (*simple)(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t,
-                          cudaStream_t s);
-    // k fused steps from t0 on a TH-row tile with an HY-row halo
-    cudaError_t (*temporal)(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
-                            int TH, int HY, cudaStream_t s);
-    int temporal_words_per_lane;  // default V of the temporal tile (tile width 32*V words)
-    int (*temporal_v_now)();      // V that `temporal` uses under the current cellato_set_temporal_width
-    int batch_words_per_lane;     // V of the batched temporal kernel
+    // one time step t (its parity selects the instantiation) with single-step kernel `variant`
+    cudaError_t (*simple)(int layout, const cellato::b200::plane_set& in, const cellato::b200::plane_set& out, int Xw,
+                          int Y, int t, int variant, cudaStream_t s);
+    // k fused steps from t0 on a TH-row tile with an HY-row halo, row loop `loop`,
+    // V words per lane (a value temporal_v returned)
+    cudaError_t (*temporal)(int layout, const cellato::b200::plane_set& in, const cellato::b200::plane_set& out,
+                            int Xw, int Y, int t0, int k, int TH, int HY, int loop, int V, cudaStream_t s);
+    // words per lane the temporal kernel runs for a requested width (0 = the rule's default)
+    int (*temporal_v)(int words_per_lane);
+    int batch_words_per_lane;  // V of the batched temporal kernel
     int temporal_warps;
     // reads and clears the count of bounded waits that gave up (device-side)
     cudaError_t (*take_wait_timeouts)(unsigned* count);
-    // batched temporal launch over a work list (see temporal_batch_kernel);
-    // prepare_batch sets the kernel's shared-memory limit (call outside capture)
+    // batched temporal kernel (see temporal_batch_kernel); prepare_batch sets
+    // the kernel's shared-memory limit (call outside capture)
     cudaError_t (*prepare_batch)(int layout, int TH);
-    cudaError_t (*temporal_batch)(int layout, const batch_grid_desc* grids, const batch_item* items, int n_items,
-                                  int parity, int t0, int TH, int HY, int ctas, cudaStream_t s);
+    // one persistent launch over a work list of every round (queue head and
+    // per-grid finished-tile counts zeroed by the caller, stream-ordered)
+    cudaError_t (*temporal_batch)(int layout, const cellato::b200::batch_grid_desc* grids,
+                                  const cellato::b200::batch_item* items, int n_items, int parity, int t0, int TH,
+                                  int HY, unsigned* head, unsigned* done, int ctas, cudaStream_t s);
     // resident CTAs per SM of the batched kernel with a TH-row tile (after prepare_batch)
     int (*batch_blocks_per_sm)(int layout, int TH);
     // state value of each dictionary index (index_to_state), 0 past `states`
     long long state_values[32];
 };
+
+namespace cellato::b200 {
+
+using rule_ops = ::cellato_rule_ops_st;
 
 // Words per lane of the single-step kernel: as wide as registers allow.  A row
 // of features costs about 3 words per plane plus 5 per count target per lane
@@ -131,20 +138,20 @@ struct rule_kernels {
 
     static cudaError_t take_wait_timeouts(unsigned* count) {
         unsigned zero = 0;
-        cudaError_t e = cudaMemcpyFromSymbol(count, g_stream_wait_timeouts, sizeof(unsigned));
+        cudaError_t e = cudaMemcpyFromSymbol(count, g_wait_timeouts, sizeof(unsigned));
         if (e != cudaSuccess) return e;
-        return cudaMemcpyToSymbol(g_stream_wait_timeouts, &zero, sizeof(unsigned));
+        return cudaMemcpyToSymbol(g_wait_timeouts, &zero, sizeof(unsigned));
     }
 
     template <int LAYOUT>
-    static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t,
+    static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t, int variant,
                                      cudaStream_t s) {
         if constexpr (LAYOUT == LAYOUT_LINEAR) {
-            const int variant = simple_variant();
             const bool stream_ok = Xw % 4 == 0;
-            // default: streaming for rules with three or more planes, whose
+            // default: streaming for rules with two or more planes, whose
             // register bands would otherwise cap occupancy
-            const bool use_stream = stream_ok && (variant == 2 || (variant == 0 && NB >= 2));
+            const bool use_stream =
+                stream_ok && (variant == SIMPLE_STREAM || (variant == SIMPLE_AUTO && NB >= 2));
             if (use_stream) return simple_stream(in, out, Xw, Y, t, s);
         }
         constexpr int VMAX = simple_words_per_lane<net, NB, LAYOUT>();
@@ -156,11 +163,11 @@ struct rule_kernels {
     }
 
     static cudaError_t simple(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t,
-                              cudaStream_t s) {
+                              int variant, cudaStream_t s) {
         switch (layout) {
-            case LAYOUT_LINEAR: return simple_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t, s);
-            case LAYOUT_TILED4: return simple_layout<LAYOUT_TILED4>(in, out, Xw, Y, t, s);
-            case LAYOUT_TILED8: return simple_layout<LAYOUT_TILED8>(in, out, Xw, Y, t, s);
+            case LAYOUT_LINEAR: return simple_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t, variant, s);
+            case LAYOUT_TILED4: return simple_layout<LAYOUT_TILED4>(in, out, Xw, Y, t, variant, s);
+            case LAYOUT_TILED8: return simple_layout<LAYOUT_TILED8>(in, out, Xw, Y, t, variant, s);
         }
         return cudaErrorInvalidValue;
     }
@@ -169,25 +176,15 @@ struct rule_kernels {
     // others (the narrower tile lets three CTAs of 200-256 rows share an SM;
     // with those heights, on B200 at 16384^2 and k = 16, 3-13% faster than two
     // words per lane and 128 interior rows for the rules of two to five planes)
-    static int temporal_v_now() {
-        const int w = temporal_width();
-        if (TEMPORAL_V == 1 || w == 1) return 1;
-        return (w == 2 || NB == 1) ? 2 : 1;
-    }
-
-    template <int LAYOUT>
-    static cudaError_t temporal_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
-                                       int TH, int HY, cudaStream_t s) {
-        if constexpr (TEMPORAL_V == 2) {
-            if (temporal_v_now() == 2) return temporal_launch<LAYOUT, 2>(in, out, Xw, Y, t0, k, TH, HY, s);
-        }
-        return temporal_launch<LAYOUT, 1>(in, out, Xw, Y, t0, k, TH, HY, s);
+    static int temporal_v(int words_per_lane) {
+        if (TEMPORAL_V == 1 || words_per_lane == 1) return 1;
+        return (words_per_lane == 2 || NB == 1) ? 2 : 1;
     }
 
     template <int LAYOUT, int V>
     static cudaError_t temporal_launch(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
-                                       int TH, int HY, cudaStream_t s) {
-        auto kern = temporal_variant() == 1 ? temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, false>
+                                       int TH, int HY, int loop, cudaStream_t s) {
+        auto kern = loop == LOOP_ROW_BY_ROW ? temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, false>
                                             : temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, true>;
         const size_t smem = (size_t)NB * TH * 32 * V * sizeof(word);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -198,12 +195,21 @@ struct rule_kernels {
         return cudaGetLastError();
     }
 
+    template <int LAYOUT>
+    static cudaError_t temporal_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
+                                       int TH, int HY, int loop, int V, cudaStream_t s) {
+        if constexpr (TEMPORAL_V == 2) {
+            if (V == 2) return temporal_launch<LAYOUT, 2>(in, out, Xw, Y, t0, k, TH, HY, loop, s);
+        }
+        return temporal_launch<LAYOUT, 1>(in, out, Xw, Y, t0, k, TH, HY, loop, s);
+    }
+
     static cudaError_t temporal(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
-                                int TH, int HY, cudaStream_t s) {
+                                int TH, int HY, int loop, int V, cudaStream_t s) {
         switch (layout) {
-            case LAYOUT_LINEAR: return temporal_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t0, k, TH, HY, s);
-            case LAYOUT_TILED4: return temporal_layout<LAYOUT_TILED4>(in, out, Xw, Y, t0, k, TH, HY, s);
-            case LAYOUT_TILED8: return temporal_layout<LAYOUT_TILED8>(in, out, Xw, Y, t0, k, TH, HY, s);
+            case LAYOUT_LINEAR: return temporal_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t0, k, TH, HY, loop, V, s);
+            case LAYOUT_TILED4: return temporal_layout<LAYOUT_TILED4>(in, out, Xw, Y, t0, k, TH, HY, loop, V, s);
+            case LAYOUT_TILED8: return temporal_layout<LAYOUT_TILED8>(in, out, Xw, Y, t0, k, TH, HY, loop, V, s);
         }
         return cudaErrorInvalidValue;
     }
@@ -247,18 +253,22 @@ struct rule_kernels {
     }
 
     static cudaError_t temporal_batch(int layout, const batch_grid_desc* grids, const batch_item* items, int n_items,
-                                      int parity, int t0, int TH, int HY, int ctas, cudaStream_t s) {
+                                      int parity, int t0, int TH, int HY, unsigned* head, unsigned* done, int ctas,
+                                      cudaStream_t s) {
         const size_t smem = tile_smem(TH);
         const dim3 block(TEMPORAL_WARPS * 32), grid(ctas);
         switch (layout) {
             case LAYOUT_LINEAR:
-                batch_kernel<LAYOUT_LINEAR>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY);
+                batch_kernel<LAYOUT_LINEAR>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY,
+                                                                        head, done);
                 break;
             case LAYOUT_TILED4:
-                batch_kernel<LAYOUT_TILED4>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY);
+                batch_kernel<LAYOUT_TILED4>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY,
+                                                                        head, done);
                 break;
             case LAYOUT_TILED8:
-                batch_kernel<LAYOUT_TILED8>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY);
+                batch_kernel<LAYOUT_TILED8>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY,
+                                                                        head, done);
                 break;
             default:
                 return cudaErrorInvalidValue;
@@ -267,15 +277,24 @@ struct rule_kernels {
     }
 
     static rule_ops ops() {
-        rule_ops o{A::name, NB, dict::number_of_values, &simple, &temporal, TEMPORAL_V, &temporal_v_now, BATCH_V,
-                   TEMPORAL_WARPS,
-                   &take_wait_timeouts, &prepare_batch, &temporal_batch, &batch_blocks_per_sm, {}};
+        rule_ops o{CELLATO_RULE_OPS_ABI, (int)sizeof(rule_ops), A::name, NB, dict::number_of_values, &simple,
+                   &temporal, &temporal_v, BATCH_V, TEMPORAL_WARPS, &take_wait_timeouts, &prepare_batch,
+                   &temporal_batch, &batch_blocks_per_sm, {}};
         static_assert(dict::number_of_values <= 32, "state table holds 32 values");
         for (int i = 0; i < dict::number_of_values; ++i)
             o.state_values[i] = static_cast<long long>(dict::index_to_state(i));
         return o;
     }
 };
+
+// The kernel table of a rule config (members name, state_dictionary,
+// algorithm, as the reference's src/<automaton>/config.hpp), instantiated in
+// the calling translation unit; the table lives until the process exits.
+template <class Config>
+const rule_ops* custom_rule_ops() {
+    static const rule_ops o = rule_kernels<Config>::ops();
+    return &o;
+}
 
 }  // namespace cellato::b200
 

@@ -80,7 +80,8 @@ private:
     void advance(int steps) {
         int in_b = 0;
         utils::check(cellato_run_simple(utils::rule_id<evaluator_type>(), CELLATO_LAYOUT_BIT_PLANES, 32,
-                                        in_b_ ? b_ : a_, in_b_ ? a_ : b_, X_, Y_, t_, steps, nullptr, &in_b),
+                                        in_b_ ? b_ : a_, in_b_ ? a_ : b_, X_, Y_, t_, steps, /*tune=*/nullptr,
+                                        /*stream=*/nullptr, &in_b),
                      "cellato_run_simple");
         if (in_b) in_b_ = !in_b_;
         t_ += steps;

@@ -74,7 +74,7 @@ private:
         int in_b = 0;
         utils::check(cellato_run_simple(utils::rule_id<evaluator_type>(), grid_t::cellato_layout, int(sizeof(word_t) * 8),
                                         pin, pout, (int)final_->x_size_original(), (int)final_->y_size_original(), t_,
-                                        steps, nullptr, &in_b),
+                                        steps, /*tune=*/nullptr, /*stream=*/nullptr, &in_b),
                      "cellato_run_simple");
         if (in_b) final_ = other;
         t_ += steps;

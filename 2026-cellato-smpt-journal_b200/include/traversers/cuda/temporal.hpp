@@ -92,9 +92,12 @@ private:
         void* pout[grid_t::needed_bits];
         for (int p = 0; p < grid_t::needed_bits; ++p) pin[p] = in[p], pout[p] = out[p];
         int in_b = 0;
+        cellato_tune tune{};
+        tune.tile_rows = tile_rows_;
         const int rc = cellato_run_temporal(utils::rule_id<evaluator_type>(), grid_t::cellato_layout,
                                             int(sizeof(word_t) * 8), pin, pout, (int)final_->x_size_original(),
-                                            (int)final_->y_size_original(), t_, steps, k_, tile_rows_, nullptr, &in_b);
+                                            (int)final_->y_size_original(), t_, steps, k_, &tune, /*stream=*/nullptr,
+                                            &in_b);
         if (rc == CELLATO_ESMEM)
             throw std::runtime_error("Configuration exceeds maximum shared memory size. The temporal tile is too large.");
         utils::check(rc, "cellato_run_temporal");

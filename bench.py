@@ -15,6 +15,20 @@ input planes from pinned host memory, runs, and downloads the result planes.
 The ping-pong plane buffers (WireWorld 128 MiB, Greenberg-Hastings 192 MiB)
 exceed the 126 MB L2, so no L2 flush is inserted between steps.
 
+The default run (--workload all) prints ONE line: the config-2 workload above
+is its headline (`value`, `e2e`, rooflines, CPU baseline), and three objects
+beside it carry the other workloads of the benchmark, each measured in the
+same process after the previous one's memory is released:
+  config3  cyclic + HPP fluid, one 32768 x 32768 bit_planes grid each, 256
+           steps; GCUPS, the single-step kernels' HBM roofline and the
+           temporal kernels' ALU roofline;
+  batched  4096 mixed grids in one CUDA-graph launch against the same grids
+           run with plain per-grid launches (ratio, bit-exactness);
+  served   a Poisson request stream through the continuous-batching server
+           against the same stream served one request at a time with
+           per-grid launches (p50 / p99 latency, GCUPS, completed vs offered).
+--workload config2|config3|batched|served prints that workload's own line.
+
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 For N > 1 run under torch.distributed.run: every rank runs the same workload on
@@ -46,26 +60,59 @@ CPU_SAMPLE_SIZE = 2048
 # DRAM bytes (read + write) per launch measured by one ncu capture of the same
 # configuration (summaries in profiles/); keyed by (rule, mode, k, size).  The
 # tile height and row loop change the re-read halo by about 1%, so one capture
-# per k stands for them.
+# per k stands for them.  Each entry names the hash of the rule's kernel
+# sources it was captured from (kernel_source_hash); an entry whose hash no
+# longer matches the sources is reported as stale and not used.
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 8, 16384): (84.97e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md"),
-    ("wire", "temporal", 16, 16384): (82.89e6, "profiles/temporal_kernel_wire_tiled64_16384_k16.md"),
-    ("excitable", "temporal", 16, 16384): (151.17e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md"),
-    ("cyclic", "temporal", 16, 32768): (1295.33e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md"),
-    ("fluid", "temporal", 16, 32768): (1028.18e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md"),
+    ("wire", "temporal", 8, 16384): (84.97e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md", None),
+    ("wire", "temporal", 16, 16384): (82.89e6, "profiles/temporal_kernel_wire_tiled64_16384_k16.md", None),
+    ("excitable", "temporal", 16, 16384): (151.17e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md", None),
+    ("cyclic", "temporal", 16, 32768): (1295.33e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md", None),
+    ("fluid", "temporal", 16, 32768): (1028.18e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md", None),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
 # temporal kernel configuration, from one ncu capture of that configuration
 # (summary in profiles/); keyed by (rule, layout, k, tile_rows, row loop, words
-# per lane, size), tile_rows 0 being the library's default height.  Each configuration is timed live and set against the ALU
-# pipe's measured rate (cellato_lop3_rate) for the compute roofline.
+# per lane, size), tile_rows 0 being the library's default height.  Each
+# configuration is timed live and set against the ALU pipe's measured rate
+# (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 16, 0, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md"),
-    ("excitable", 1, 16, 0, 2, 1, 16384): (70207344, "profiles/alu_pipe_temporal_kernels.md"),
-    ("cyclic", 0, 16, 0, 2, 1, 32768): (1664571440, "profiles/alu_pipe_temporal_kernels.md"),
-    ("fluid", 0, 16, 0, 2, 1, 32768): (312104380, "profiles/alu_pipe_temporal_kernels.md"),
+    ("wire", 1, 16, 0, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("excitable", 1, 16, 0, 2, 1, 16384): (70207344, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("cyclic", 0, 16, 0, 2, 1, 32768): (1664571440, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("fluid", 0, 16, 0, 2, 1, 32768): (312104380, "profiles/alu_pipe_temporal_kernels.md", None),
 }
+
+AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
+                  "brian": "brian", "maze": "maze", "cyclic": "cyclic", "fluid": "fluid", "critters": "critters",
+                  "traffic": "traffic"}
+
+
+def kernel_source_hash(rule: str) -> str:
+    """First 16 hex digits of the SHA-256 of everything a rule's kernels are
+    compiled from: the lowering, the engine, the launchers, the rule's own
+    headers and the build flags."""
+    import hashlib
+    files = [os.path.join(PKG, "include", "b200", f) for f in ("lower.cuh", "engine.cuh", "rule_kernels.cuh")]
+    d = os.path.join(PKG, "automata", AUTOMATON_DIRS[rule])
+    files += sorted(os.path.join(d, f) for f in os.listdir(d))
+    files.append(os.path.join(PKG, "Makefile"))
+    h = hashlib.sha256()
+    for f in files:
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def measured(table: dict, key, rule: str):
+    """(value, source, fresh) of a capture, fresh = captured from the current
+    kernel sources; None when there is no capture of this configuration."""
+    e = table.get(key)
+    if e is None:
+        return None
+    value, src, digest = e
+    return value, src, digest is not None and digest == kernel_source_hash(rule)
 
 
 def parse():
@@ -82,8 +129,9 @@ def parse():
     ap.add_argument("--choice", default="", help="pin the traverser per automaton instead of autotuning, "
                                                  "e.g. wire=temporal:8:128:1,excitable=temporal:16:0:2:1 "
                                                  "(mode:k:tile_rows:loop:words_per_lane)")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "batched", "served"],
-                    help="config2: WireWorld + Greenberg-Hastings 16384^2 x 1000 steps (default); "
+    ap.add_argument("--workload", default="all", choices=["all", "config2", "config3", "batched", "served"],
+                    help="all (default): the config2 line with config3, batched and served beside it; "
+                         "config2: WireWorld + Greenberg-Hastings 16384^2 x 1000 steps; "
                          "config3: cyclic + HPP fluid 32768^2 x 256 steps on bit_planes, with the single-step "
                          "kernels' HBM roofline beside the autotuned run; "
                          "batched: many mixed grids in one CUDA-graph launch vs per-grid launches; "
@@ -114,12 +162,14 @@ SINGLE_GRID_WORKLOADS = {
 K_MAX = 16
 
 
-def apply_workload(args) -> None:
-    """Sets the automata, sizes and layout of a single-grid workload."""
+def apply_workload(args, name=None) -> None:
+    """Sets the automata, sizes and layout of a single-grid workload (the
+    config2 ones for the batched and served workloads, whose layout and word
+    size they share)."""
     global AUTOMATA, LAYOUT, K_MAX
-    automata, side, steps, layout, kmax = SINGLE_GRID_WORKLOADS.get(args.workload, SINGLE_GRID_WORKLOADS["config2"])
-    if args.workload in SINGLE_GRID_WORKLOADS:
-        AUTOMATA, LAYOUT, K_MAX = automata, layout, kmax
+    name = name or args.workload
+    automata, side, steps, layout, kmax = SINGLE_GRID_WORKLOADS.get(name, SINGLE_GRID_WORKLOADS["config2"])
+    AUTOMATA, LAYOUT, K_MAX = automata, layout, kmax
     args.size = args.size or side
     args.ca_steps = args.ca_steps or steps
 
@@ -306,7 +356,8 @@ def workload_config(args, extra=None):
 
 
 # ------------------------------------------------------------- our arm
-def our_arm(args, rank: int, world: int):
+def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
+    """The single-grid workload set by apply_workload; returns its line."""
     import numpy as np
     import torch
     from cellato_b200 import autotune, inputs, lib, replicas
@@ -514,10 +565,11 @@ def our_arm(args, rank: int, world: int):
            "peak": round(lib.lop3_rate(sp) / 1e9, 1),
            "peak_source": "measured live: cellato_lop3_rate (independent lop3.b32 chains, full occupancy)",
            "kernels": {}}
-    for key, (count, src) in MEASURED_ALU.items():
+    for key in MEASURED_ALU:
         a, lay, k, th, loop, width, size = key
         if a not in grids or lay != LAYOUT or size != args.size:
             continue
+        count, src, fresh = measured(MEASURED_ALU, key, a)
         g = grids[a]
         c = {"mode": "temporal", "k": k, "tile_rows": th, "loop": loop, "width": width}
         nl = 8
@@ -531,8 +583,10 @@ def our_arm(args, rank: int, world: int):
         alu["kernels"][a] = {"kernel": describe_choice(c),
                              "timed_choice": all(g["choice"].get(n) == v for n, v in c.items()),
                              "alu_warp_insts_per_launch": count, "ms_per_launch": round(msl, 4),
-                             "achieved": round(ach, 1), "frac": round(ach / alu["peak"], 4),
-                             "alu_ops_per_cell_step": round(count * 32 / (X * Y * k), 2), "source": src}
+                             "achieved": round(ach, 1) if fresh else None,
+                             "frac": round(ach / alu["peak"], 4) if fresh else None,
+                             "alu_ops_per_cell_step": round(count * 32 / (X * Y * k), 2), "source": src,
+                             "capture_matches_kernel_sources": fresh}
         g["a"].buf.copy_(g["init"].buf)
     torch.cuda.synchronize()
 
@@ -544,10 +598,11 @@ def our_arm(args, rank: int, world: int):
     bytes_per_launch = 2 * g["nb"] * g["init"].plane_bytes  # read + write every plane once per launch
     achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9
     peak = peaks["hbm_gbs"]
-    measured = MEASURED_TRAFFIC.get((dom, g["choice"]["mode"], g["choice"]["k"], args.size))
+    cap = measured(MEASURED_TRAFFIC, (dom, g["choice"]["mode"], g["choice"]["k"], args.size), dom)
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": measured[0] if measured else None,
-            "traffic_source": measured[1] if measured else "no capture of this configuration",
+            "frac": round(achieved / peak, 4), "traffic": cap[0] if cap and cap[2] else None,
+            "traffic_source": (cap[1] if cap[2] else f"{cap[1]} (stale: captured from older kernel sources)")
+            if cap else "no capture of this configuration",
             "kernel": f"{'temporal_kernel' if g['choice']['mode'] == 'temporal' else g['choice']['mode']} "
                       f"({dom}, k={g['choice']['k']})",
             "peak_source": peaks["source"],
@@ -556,9 +611,9 @@ def our_arm(args, rank: int, world: int):
             "single_step_equivalent_frac": round(per_gcups[dom] * 1e9 * g["nb"] / 4 / 1e9 / peak, 4)}
 
     if rank != 0:
-        return
+        return None
     cpu = None
-    if not args.no_cpu_baseline:
+    if cpu_baseline and not args.no_cpu_baseline:
         kind, run = load_reference_cpu()
         th = host_threads()
         v, sample = cpu_sample(run, th, target_s=10.0)
@@ -587,7 +642,7 @@ def our_arm(args, rank: int, world: int):
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ------------------------------------------------------- batched workload
@@ -692,7 +747,7 @@ def batched_arm(args, rank: int, world: int):
     per_grid_launches = sum(-(-s // ks[r]) for r, _, _, s in specs)
 
     if rank != 0:
-        return
+        return None
     value = cells_total * world / (ms_batched * 1e-3) / 1e9
     per_grid = cells_total / (ms_per_grid * 1e-3) / 1e9
     line = {
@@ -714,7 +769,7 @@ def batched_arm(args, rank: int, world: int):
         "gpu_launches": info["kernel_launches"] * args.steps,
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def tune_temporal_k(dev, layout: int, W: int, sides) -> dict:
@@ -774,9 +829,11 @@ def served_arm(args, rank: int, world: int):
     ks = tune_temporal_k(dev, layout, W, {r: (1024, 1024) for r in range(10)})
     torch.cuda.synchronize()
 
-    # ---- served
+    # ---- served; the plane pool may use 80% of the memory free now
+    free_b, _ = torch.cuda.mem_get_info(dev)
+    cap = int(0.8 * free_b)
     with ClockSampler(dev.index) as clocks:
-        srv = Server(layout, W, k_per_rule=ks)
+        srv = Server(layout, W, hbm_cap_bytes=cap, k_per_rule=ks)
         lat, sums, ids = {}, {}, {}
         keep = set(sample)
         i = 0
@@ -838,7 +895,7 @@ def served_arm(args, rank: int, world: int):
                 "checksum_mismatches_vs_served": mism}
 
     if rank != 0:
-        return
+        return None
     lats = np.array([lat[j] for j in range(n)])
     value = cell_updates * world / makespan / 1e9
     line = {
@@ -852,8 +909,14 @@ def served_arm(args, rank: int, world: int):
                    "k_per_automaton": {inputs.RULES[r]: k for r, k in ks.items()},
                    "quantisation": "X to a multiple of 64, Y to a multiple of 16",
                    "cell_updates": cell_updates,
+                   "hbm_cap_bytes": cap,
                    "offered_gcups": round(cell_updates / args.serve_seconds / 1e9, 1),
                    "timing": "host wall clock from the first scheduled arrival to the last result"},
+        "requests": {"offered": n, "completed": int(len(lat)),
+                     "offered_gcups": round(cell_updates / args.serve_seconds / 1e9, 1),
+                     "completed_gcups": round(value, 1),
+                     "note": "every offered request completes; the offered load exceeds one GPU's rate, so the "
+                             "queue and the latency grow with the arrival window"},
         "latency_ms": {"p50": round(1e3 * float(np.percentile(lats, 50)), 1),
                        "p99": round(1e3 * float(np.percentile(lats, 99)), 1),
                        "max": round(1e3 * float(lats.max()), 1)},
@@ -867,7 +930,7 @@ def served_arm(args, rank: int, world: int):
         "gpu_launches": stats["kernel_launches"],
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def measured_peaks():
@@ -885,6 +948,48 @@ def max_over_ranks(ms: float, world: int) -> float:
     return replicas.max_over_ranks(ms) if world > 1 else ms
 
 
+def _free_device_memory():
+    import gc
+    import torch
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+
+def _sub(line, keys):
+    """The keys of a workload's own line kept beside the headline."""
+    return {k: line[k] for k in keys if k in line}
+
+
+def all_workloads(args, rank: int, world: int):
+    """The config2 line with config3, batched and served beside it."""
+    import copy
+    apply_workload(args, "config2")
+    line = our_arm(args, rank, world)
+    _free_device_memory()
+    a3 = copy.copy(args)
+    a3.size = a3.ca_steps = None
+    a3.choice = ""
+    apply_workload(a3, "config3")
+    c3 = our_arm(a3, rank, world, cpu_baseline=False)
+    _free_device_memory()
+    apply_workload(args, "config2")
+    bt = batched_arm(args, rank, world)
+    _free_device_memory()
+    sv = served_arm(args, rank, world)
+    _free_device_memory()
+    if rank != 0:
+        return
+    line["config3"] = _sub(c3, ["value", "unit", "ms_per_step", "config", "per_automaton_gcups", "e2e",
+                                "gpu_launches", "roofline", "single_step_roofline", "alu_roofline", "clocks"])
+    line["batched"] = _sub(bt, ["value", "unit", "ms_per_step", "steps", "config", "per_grid_launches_gcups",
+                                "batched_over_per_grid", "per_grid_kernel_launches", "bit_exact_vs_per_grid",
+                                "mismatching_grids", "gpu_launches", "clocks"])
+    line["served"] = _sub(sv, ["value", "unit", "config", "requests", "latency_ms", "per_grid",
+                               "served_over_per_grid", "sample_bit_exact", "server", "e2e", "gpu_launches", "clocks"])
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     from cellato_b200 import replicas
@@ -892,12 +997,13 @@ def main():
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)
-        elif args.workload == "batched":
-            batched_arm(args, rank, world)
-        elif args.workload == "served":
-            served_arm(args, rank, world)
+        elif args.workload == "all":
+            all_workloads(args, rank, world)
         else:
-            our_arm(args, rank, world)
+            fn = {"batched": batched_arm, "served": served_arm}.get(args.workload, our_arm)
+            line = fn(args, rank, world)
+            if line is not None:
+                print(json.dumps(line), flush=True)
     finally:
         replicas.shutdown()
 

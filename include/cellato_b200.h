@@ -56,7 +56,9 @@ typedef enum {
     CELLATO_LAYOUT_TILED_BIT_PLANES = 1
 } cellato_layout;
 
-/* Rule ids: the ten automata of the reference (src/<automaton>/config.hpp). */
+/* Rule ids of the ten automata of the reference (src/<automaton>/config.hpp),
+ * built into the library.  Rules registered with cellato_rule_register get
+ * the ids that follow (CELLATO_BUILTIN_RULES, CELLATO_BUILTIN_RULES + 1, ...). */
 typedef enum {
     CELLATO_GAME_OF_LIFE = 0,
     CELLATO_FOREST_FIRE = 1,
@@ -68,8 +70,33 @@ typedef enum {
     CELLATO_FLUID = 7,
     CELLATO_CRITTERS = 8,
     CELLATO_TRAFFIC = 9,
-    CELLATO_RULE_COUNT = 10
+    CELLATO_BUILTIN_RULES = 10
 } cellato_rule;
+
+/* Capacity of the rule table: the built-in rules plus registered ones. */
+#define CELLATO_MAX_RULES 256
+
+/* Kernel table of one rule (opaque to C).  A C++ translation unit compiled
+ * with nvcc for sm_100a builds one for any rule written in the rule DSL with
+ * cellato::b200::custom_rule_ops<Config>() (2026-cellato-smpt-journal_b200/
+ * include/b200/custom_rule.cuh); the library runs it through every entry point
+ * once it is registered. */
+typedef struct cellato_rule_ops_st cellato_rule_ops;
+
+/* Per-call tuning of the traversers; NULL or all-zero fields = the library's
+ * choices.  The reference passes the same kind of knobs per run in run_params
+ * (include/experiments/run_params.hpp:10-43: cuda_block_size_y,
+ * temporal_tile_size_y); here they select among this library's kernels.  Every
+ * choice gives the same results. */
+typedef struct {
+    int simple_kernel;   /* single-step kernel, linear layout: 0 automatic, 1 register bands, 2 bulk-copy
+                            streaming (rows of 16-byte multiples; others use 1) */
+    int row_loop;        /* temporal row loop: 0 automatic, 1 row by row, 2 the input rows of each three-row
+                            trip read before its in-place writes */
+    int words_per_lane;  /* temporal tile width: 0 the rule's default (2 for one-plane rules, else 1), 1, or 2
+                            (rules of up to three planes; others use 1); the tile is 32 x this many words */
+    int tile_rows;       /* temporal tile rows including both k-row halos; 0 the library's default */
+} cellato_tune;
 
 /* ---- identity ----------------------------------------------------------- */
 
@@ -80,7 +107,7 @@ const char* cellato_version(void);
 const char* cellato_last_error(void);
 
 /* Rule id of a CLI automaton name ("game-of-life", "fire" or "forest-fire",
- * ...; src/main.cpp:55-77), or -1. */
+ * ...; src/main.cpp:55-77) or of a registered rule's name, or -1. */
 int cellato_rule_from_name(const char* name);
 
 /* Name of a rule id (the config's `name`, e.g. "forest-fire"), or NULL. */
@@ -91,6 +118,18 @@ int cellato_rule_planes(int rule);
 
 /* number_of_values of the rule's state dictionary, or -1. */
 int cellato_rule_states(int rule);
+
+/* Number of rule ids in use: CELLATO_BUILTIN_RULES plus the registered rules. */
+int cellato_rule_count(void);
+
+/* Adds a rule to the library's rule table and returns its id in *rule_out
+ * (the next free id).  `ops` must stay valid until the process exits (the
+ * table custom_rule_ops returns does).  CELLATO_EINVAL for a table built
+ * against another layout of cellato_rule_ops, a name already in use or a full
+ * table.  Registering the same table twice returns its first id.  Thread-safe;
+ * ids are never reused.  Replaces the reference's per-automaton explicit
+ * instantiation in src/_shared/cuda_instantiation_template.cuh:77-193. */
+int cellato_rule_register(const cellato_rule_ops* ops, int* rule_out);
 
 /* Bytes of one plane of an X x Y grid (X*Y/8). */
 size_t cellato_plane_bytes(int x_cells, int y_cells);
@@ -128,46 +167,22 @@ int cellato_unpack_cells(int layout, int word_bits, int nb, const void* const* p
 /* Simple traverser (replaces include/traversers/cuda/simple.cu:43-87 with
  * process_grid_kernel_simple :20-39): `steps` single-step launches, ping-pong
  * between planes_a (input) and planes_b.  *result_in_b is set to 1 when the
- * final state is in planes_b (odd number of launches), else 0.  Nothing is
+ * final state is in planes_b (odd number of launches), else 0.  tune: NULL or
+ * its simple_kernel field (the other fields are ignored).  Nothing is
  * allocated; planes_a and planes_b must not overlap. */
 int cellato_run_simple(int rule, int layout, int word_bits, void* const* planes_a, void* const* planes_b,
-                       int x_cells, int y_cells, int t0, int steps, cellato_stream_t stream, int* result_in_b);
+                       int x_cells, int y_cells, int t0, int steps, const cellato_tune* tune,
+                       cellato_stream_t stream, int* result_in_b);
 
 /* Temporal traverser (replaces include/traversers/cuda/temporal.cu:137-272
  * with process_grid_kernel_linear_temporal :35-135): launches of k fused steps
- * each (the last launch takes the remainder), ping-pong as above.
- * k in 1..32; tile_rows = rows of the shared-memory tile including the 2*k-row
- * halo (0 = the library's choice for this rule/layout).  Returns CELLATO_ESMEM
- * when the tile does not fit ("temporal tile is too large" in the reference,
- * temporal.cu:214-216). */
+ * each (the last launch takes the remainder), ping-pong as above.  k in 1..32.
+ * tune: NULL or its row_loop, words_per_lane and tile_rows fields.  Returns
+ * CELLATO_ESMEM when the tile does not fit ("temporal tile is too large" in
+ * the reference, temporal.cu:214-216). */
 int cellato_run_temporal(int rule, int layout, int word_bits, void* const* planes_a, void* const* planes_b,
-                         int x_cells, int y_cells, int t0, int steps, int k, int tile_rows,
+                         int x_cells, int y_cells, int t0, int steps, int k, const cellato_tune* tune,
                          cellato_stream_t stream, int* result_in_b);
-
-/* Selects the single-step kernel used for the linear layout: 0 = automatic,
- * 1 = register-band kernel, 2 = bulk-copy streaming kernel (rows of 16-byte
- * multiples only; others fall back to 1).  Process-wide, not synchronised with
- * concurrent launches; the autotuner sweeps it.  No counterpart in the
- * reference (one simple kernel). */
-int cellato_set_simple_variant(int variant);
-
-/* Selects the row loop of the temporal kernel (cellato_run_temporal): 0 =
- * automatic, 1 = each row read just before the row above it is evaluated, 2 =
- * the input rows of each three-row trip read before the trip's in-place writes.
- * Same results; the speed depends on the rule.  Process-wide, not synchronised
- * with concurrent launches; the autotuner sweeps it.  No counterpart in the
- * reference (one temporal kernel). */
-int cellato_set_temporal_variant(int variant);
-
-/* Words per lane of the temporal kernel (cellato_run_temporal): 0 = the
- * library's default (2 for one-plane rules, else 1), 1 = one word per lane
- * (half the registers and shared memory per tile row, so more CTAs per SM),
- * 2 = two (rules of up to three planes; others use one).  Same results; the
- * tile is 32 x words-per-lane words wide, so default tile heights and
- * cellato_temporal_max_tile_rows follow the setting.  Process-wide, not
- * synchronised with concurrent launches; the autotuner sweeps it.  No
- * counterpart in the reference. */
-int cellato_set_temporal_width(int words_per_lane);
 
 /* Reads and clears the number of bounded device-side waits (mbarrier waits of
  * the streaming single-step kernel) that gave up since the last call; returns
@@ -190,13 +205,15 @@ typedef struct {
 } cellato_batch_grid;
 
 /* Plans a batch: grids of one rule advance k_per_rule[rule] steps per round
- * (NULL or 0 entries: 8), one batched launch per round covers every tile of
- * every grid of that rule still running, the rules' chains of rounds become
- * parallel branches of one CUDA graph (built and instantiated here).  Allocates
- * the work lists on the device.  Grids steps count from 0 (step parity as a run
- * with t0 = 0). */
+ * (k_per_rule has n_k_per_rule entries; NULL, 0 or missing entries: 8).  All
+ * rounds of all grids of one rule are ONE persistent kernel launch, in which a
+ * grid's next round starts as soon as its previous round is done; the rules'
+ * launches are parallel branches of one CUDA graph (built and instantiated
+ * here).  Allocates the work lists on the device.  Grids' steps count from 0
+ * (step parity as a run with t0 = 0).  A bounded device wait of the persistent
+ * kernel that gives up is counted by cellato_device_wait_timeouts. */
 int cellato_batch_create(int layout, int word_bits, const cellato_batch_grid* grids, int n_grids,
-                         const int* k_per_rule, cellato_batch_t* out);
+                         const int* k_per_rule, int n_k_per_rule, cellato_batch_t* out);
 /* One graph launch: every grid advances its `steps` (ping-pong a -> b -> ...). */
 int cellato_batch_launch(cellato_batch_t batch, cellato_stream_t stream);
 /* 1 when grid's result is in planes_b after a launch (odd number of rounds). */
@@ -215,26 +232,32 @@ int cellato_batch_destroy(cellato_batch_t batch);
  * memory (CELLATO_NOALLOC_MAX_GRIDS descriptors and CELLATO_NOALLOC_MAX_ITEMS
  * work items, about 1.2 MB, held by every GPU that loads the library until the
  * process exits) instead of a cudaMalloc'd one; no CUDA graph, stream or event
- * is created, kernels are launched in order on `stream`.  Calls no cudaMalloc or
- * cudaFree.
+ * is created, the rules' persistent kernels are launched in order on `stream`.
+ * Calls no cudaMalloc or cudaFree.
+ *   - The work list is copied from host memory the library does not pin, so
+ *     the call waits for the work already queued on `stream`; a stream being
+ *     captured into a CUDA graph is refused with CELLATO_EINVAL.
  *   - grids: as for cellato_batch_create; result_in_b: n_grids ints (host),
  *     set to 1 where a grid's result is in planes_b.
  *   - More than CELLATO_NOALLOC_MAX_GRIDS grids or CELLATO_NOALLOC_MAX_ITEMS
  *     work items (tiles x rounds over the batch): CELLATO_EINVAL, nothing runs.
  *   - The first call on a device looks up the array's device address (with
- *     cudaGetSymbolAddress); make that first call before any stream capture.
+ *     cudaGetSymbolAddress) and caches it for the process; do not use this
+ *     entry point on a device after cudaDeviceReset.
  *   - All calls share the array and it keeps the last call's work list; each
- *     call writes the whole list it uses before its kernels (stream-ordered).
+ *     call writes the whole list it uses and clears the counters its kernels
+ *     count from zero, before its kernels (stream-ordered).
  *     Calls whose work can overlap on the GPU (other streams, other threads)
  *     race on the array: serialise them. */
 #define CELLATO_NOALLOC_MAX_GRIDS 1024
 #define CELLATO_NOALLOC_MAX_ITEMS 65536
 int cellato_batch_run_noalloc(int layout, int word_bits, const cellato_batch_grid* grids, int n_grids,
-                              const int* k_per_rule, cellato_stream_t stream, int* result_in_b);
+                              const int* k_per_rule, int n_k_per_rule, cellato_stream_t stream, int* result_in_b);
 
 /* Largest tile_rows the temporal kernel accepts for (rule, layout, word_bits)
- * on the current device, or a negative status. */
-int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits);
+ * at the given words_per_lane (as cellato_tune) on the current device, or a
+ * negative status. */
+int cellato_temporal_max_tile_rows(int rule, int layout, int word_bits, int words_per_lane);
 
 /* ---- whole-grid operations ----------------------------------------------- */
 
@@ -310,10 +333,11 @@ int cellato_lop3_rate(double* lane_ops_per_second, cellato_stream_t stream);
  *     by the server holds them).
  *   - Iteration (cellato_server_iterate): the resident requests, oldest first,
  *     are activated while their temporal tiles fit in tile_budget; each active
- *     request advances up to chunk_rounds rounds of k steps.  A round is one
- *     batched temporal launch per automaton over the tiles of every active
- *     request of it, the automata on parallel streams.  Requests join and leave
- *     between iterations, at any step count.
+ *     request advances up to chunk_rounds rounds of k steps.  The rounds of
+ *     one automaton are one persistent batched launch over the tiles of every
+ *     active request of it (a request's next round starts when its previous
+ *     round is done), the automata on parallel streams.  Requests join and
+ *     leave between iterations, at any step count.
  *   - Completion: a finished request's checksum (as cellato_checksum) is
  *     computed on the device and copied back; cellato_server_poll returns it.
  *     Without `keep` its planes are freed at once; with `keep` they stay,
@@ -331,7 +355,9 @@ typedef struct {
     int tile_budget;                  /* temporal tiles per round over all active requests; 0: 32 per SM */
     int chunk_rounds;                 /* rounds per request per iteration; 0: 4 */
     int max_inflight;                 /* iterations queued on the device at once; 0: 2 */
-    int k_per_rule[10];               /* temporal depth per rule, 1..32; 0: 16 */
+    const int* k_per_rule;            /* temporal depth per rule id, 1..32 (copied at creation);
+                                         NULL, 0 or ids past n_k_per_rule: 16 */
+    int n_k_per_rule;
 } cellato_server_config;
 
 typedef struct {

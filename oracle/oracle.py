@@ -4,6 +4,8 @@
 * ``RefOracle`` -- the reference's own CPU code compiled by oracle/Makefile into
   oracle/_ref/libcellato_ref.so (present where the reference tree was available
   at build time; it travels with the repository snapshot).
+* ``RefCustomOracle`` -- the reference's standard path instantiated for the
+  custom rules of tests/cpp/custom_rules.hpp (oracle/_ref/libcellato_ref_custom.so).
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use this
 module, and only as the checker or the timed CPU baseline.  Cells are uint8
@@ -18,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libcellato_ref.so")
+REF_CUSTOM_PATH = os.path.join(HERE, "_ref", "libcellato_ref_custom.so")
 
 RULES = ["game-of-life", "forest-fire", "wire", "excitable", "brian",
          "maze", "cyclic", "fluid", "critters", "traffic"]
@@ -211,3 +214,33 @@ class RefOracle:
         if n < 0:
             raise RuntimeError("reference checksum failed")
         return buf.value.decode()
+
+
+class RefCustomOracle:
+    """The reference's CPU standard path on the custom rules (rules outside both
+    the reference and the B200 library, tests/cpp/custom_rules.hpp)."""
+
+    def __init__(self, path: str = REF_CUSTOM_PATH):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+        lib = ctypes.CDLL(path)
+        lib.cref_custom_name.restype = ctypes.c_char_p
+        lib.cref_custom_run.argtypes = [ctypes.c_int, _u8p, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        self.lib = lib
+
+    def count(self) -> int:
+        return self.lib.cref_custom_count()
+
+    def name(self, which: int) -> str:
+        return self.lib.cref_custom_name(which).decode()
+
+    def states(self, which: int) -> int:
+        return self.lib.cref_custom_states(which)
+
+    def run_standard(self, which: int, cells: np.ndarray, steps: int) -> np.ndarray:
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        Y, X = cells.shape
+        out = np.empty_like(cells)
+        if self.lib.cref_custom_run(which, _ptr(cells), _ptr(out), X, Y, steps) != 0:
+            raise RuntimeError("reference standard run of a custom rule failed")
+        return out

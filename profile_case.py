@@ -1,6 +1,7 @@
-"""Run one hot-path configuration a fixed number of times, for profilers.
+"""Run one hot-path configuration a fixed number of times, for profilers
+(the command the ncu summaries under profiles/ were made with).
 
-    python -m cellato_b200.profile_case --rule excitable --layout tiled_bit_planes \
+    python profile_case.py --rule excitable --layout tiled_bit_planes \
         --word-bits 64 --size 16384 --mode temporal --k 16 --launches 3
 
 Inputs are the seeded workload grid of the rule, packed on the device.  Each
@@ -11,11 +12,14 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
+import sys
 
 import torch
 
-from . import inputs, lib
-from .device import DevicePlanes
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "2026-cellato-smpt-journal_b200"))
+from cellato_b200 import inputs, lib  # noqa: E402
+from cellato_b200.device import DevicePlanes  # noqa: E402
 
 
 def main() -> None:
@@ -30,8 +34,9 @@ def main() -> None:
                          "(cellato_lop3_rate: one warm-up and three timed launches)")
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--tile-rows", type=int, default=0)
-    ap.add_argument("--loop", type=int, default=0, help="temporal row loop (cellato_set_temporal_variant)")
-    ap.add_argument("--width", type=int, default=0, help="temporal words per lane (cellato_set_temporal_width)")
+    ap.add_argument("--loop", type=int, default=0, help="temporal row loop (cellato_tune.row_loop)")
+    ap.add_argument("--width", type=int, default=0, help="temporal words per lane (cellato_tune.words_per_lane)")
+    ap.add_argument("--simple-kernel", type=int, default=0, help="single-step kernel (cellato_tune.simple_kernel)")
     ap.add_argument("--launches", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     a = ap.parse_args()
@@ -42,8 +47,6 @@ def main() -> None:
         return
     if a.mode == "ops":
         return ops(a, r)
-    lib.set_temporal_variant(a.loop)
-    lib.set_temporal_width(a.width)
     nb = lib.rule_planes(r)
     layout = lib.LAYOUTS[a.layout]
     X = Y = a.size
@@ -54,8 +57,9 @@ def main() -> None:
 
     def launch(n):
         if a.mode == "simple":
-            return lib.run_simple(r, layout, a.word_bits, pa.ptrs, pb.ptrs, X, Y, 0, n)
-        return lib.run_temporal(r, layout, a.word_bits, pa.ptrs, pb.ptrs, X, Y, 0, n * k, k, a.tile_rows)
+            return lib.run_simple(r, layout, a.word_bits, pa.ptrs, pb.ptrs, X, Y, 0, n, simple_kernel=a.simple_kernel)
+        return lib.run_temporal(r, layout, a.word_bits, pa.ptrs, pb.ptrs, X, Y, 0, n * k, k, a.tile_rows,
+                                row_loop=a.loop, words_per_lane=a.width)
 
     launch(a.warmup)
     torch.cuda.synchronize()

@@ -25,6 +25,8 @@ def _ensure_built():
     lib = os.path.join(PKG, "lib", "libcellato_b200.so")
     if not os.path.exists(lib):
         subprocess.run(["make", "-j8", "-C", PKG], check=True, capture_output=True)
+    # rebuilt when its sources or the package headers changed (make's own check)
+    subprocess.run(["make", "-C", os.path.join(ROOT, "tests", "cpp")], check=True, capture_output=True)
     olib = os.path.join(ROOT, "oracle", "liboracle.so")
     if not os.path.exists(olib):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True,

@@ -24,6 +24,10 @@
 
 using namespace cellato::b200::serve;
 
+// rule ids drawn by the scenarios: the ten built-in ones and three registered
+// ones; the last two have no k entry (the scheduler's default applies)
+constexpr int RULES = 13;
+
 #define CHECK(c, ...)                                   \
     do {                                                \
         if (!(c)) {                                     \
@@ -50,7 +54,8 @@ int scenario(unsigned seed, long long cap, long long budget, int chunk_rounds) {
     lim.cap_bytes = cap;
     lim.tile_budget = budget;
     lim.chunk_rounds = chunk_rounds;
-    for (int r = 0; r < RULES; ++r) lim.k[r] = 1 + (int)(rng() % 20);
+    lim.k.assign(RULES - 2, 0);
+    for (int r = 0; r < RULES - 2; ++r) lim.k[r] = 1 + (int)(rng() % 20);
     scheduler sch(lim);
     std::map<long long, truth> t;
     std::vector<long long> submitted;
@@ -63,7 +68,7 @@ int scenario(unsigned seed, long long cap, long long budget, int chunk_rounds) {
             truth q;
             q.rule = (int)(rng() % RULES);
             q.steps = (rng() % 10 == 0) ? 0 : 1 + (int)(rng() % 300);
-            q.k = lim.k[q.rule];
+            q.k = lim.k_of(q.rule);
             q.bytes = 1 + (long long)(rng() % (unsigned)(cap / 3 + 1));
             if (rng() % 50 == 0) q.bytes = cap + 5;  // larger than the cap
             q.tiles = 1 + (int)(rng() % 40);
@@ -111,7 +116,8 @@ int scenario(unsigned seed, long long cap, long long budget, int chunk_rounds) {
         CHECK(tiles <= budget || p.active.size() == 1, "tiles %lld over budget %lld with %zu active", tiles, budget,
               p.active.size());
         std::map<long long, int> rounds_here;
-        for (int r = 0; r < RULES; ++r)
+        CHECK((int)p.rounds.size() <= RULES, "rounds for %zu rule ids", p.rounds.size());
+        for (int r = 0; r < (int)p.rounds.size(); ++r)
             for (size_t q = 0; q < p.rounds[r].size(); ++q)
                 for (const round_entry& e : p.rounds[r][q]) {
                     truth& x = t[e.id];

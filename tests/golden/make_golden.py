@@ -16,6 +16,12 @@ restatement in oracle/ and the GPU path.
 * large.json  -- workload-sized cases stored as SHA-256 of the input and output
                  grids plus the reference 4x4 tile checksum string; the input is
                  regenerated from the named seeded generator and its hash checked.
+* custom.npz  -- full input/output grids of the three custom rules of
+                 tests/cpp/custom_rules.hpp (rules outside the reference and the
+                 library), run by the reference's standard path instantiated for
+                 them (oracle/_ref/libcellato_ref_custom.so).
+
+`python tests/golden/make_golden.py custom` writes custom.npz alone.
 """
 from __future__ import annotations
 
@@ -31,7 +37,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "2026-cellato-smpt-journal_b200"))
 
-from oracle import RefOracle  # noqa: E402
+from oracle import RefCustomOracle, RefOracle  # noqa: E402
 from cellato_b200 import inputs  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -80,7 +86,31 @@ def make_input(ref: RefOracle, rule: int, gen: str, X: int, Y: int, seed: int) -
     raise ValueError(gen)
 
 
+# (X, Y, steps, seed) for the custom rules: uniform random states
+CUSTOM_CASES = [(64, 8, 9, 1), (128, 64, 37, 2), (192, 24, 64, 3), (256, 256, 100, 4), (320, 48, 23, 5)]
+
+
+def make_custom() -> None:
+    ref = RefCustomOracle()
+    arrays, index = {}, []
+    for which in range(ref.count()):
+        for ci, (X, Y, steps, seed) in enumerate(CUSTOM_CASES):
+            cells = inputs.uniform(X, Y, ref.states(which), 1000 * which + seed)
+            key = f"c{which}_{ci}"
+            arrays[key + "_in"] = cells
+            arrays[key + "_out"] = ref.run_standard(which, cells, steps)
+            index.append({"key": key, "rule": ref.name(which), "which": which, "X": X, "Y": Y, "steps": steps,
+                          "seed": 1000 * which + seed})
+    arrays["index"] = np.frombuffer(json.dumps(index).encode(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "custom.npz"), **arrays)
+    print(f"custom.npz: {len(index)} cases")
+
+
 def main() -> None:
+    if sys.argv[1:] == ["custom"]:
+        make_custom()
+        return
+    make_custom()
     ref = RefOracle()
     threads = os.cpu_count() or 1
     arrays = {}

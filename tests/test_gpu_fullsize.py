@@ -7,8 +7,9 @@ the grids are seeded on the device, and kernels check one another.
   and the checksums are equal.
 * The same seeded grid run on the linear and on the tiled layout has the same
   checksum (the checksum is over cell values, not bytes).
-* Cyclic and HPP fluid on 32768 x 32768 (the bit_planes workload): temporal k=8
-  and the k=1 temporal path agree with the single-step kernel.
+* Cyclic and HPP fluid on 32768 x 32768 (the bit_planes workload): temporal
+  k = 8 ... 32 at the default tile height (what the config-3 bench times) and
+  the k = 1 temporal path agree with the single-step kernel.
 The smaller sizes are pinned to the reference by the golden fixtures; these
 tests pin the large ones to the small-size-verified kernels."""
 import numpy as np
@@ -28,16 +29,13 @@ def seeded(rule, layout, X, Y, seed):
     return a, b
 
 
-def run(rule, layout, X, Y, steps, seed, mode, k=1, tile_rows=0, loop=0):
+def run(rule, layout, X, Y, steps, seed, mode, k=1, tile_rows=0, loop=0, width=0, simple_kernel=0):
     a, b = seeded(rule, layout, X, Y, seed)
-    lib.set_temporal_variant(loop)
-    try:
-        if mode == "simple":
-            in_b = lib.run_simple(rule, layout, 64, a.ptrs, b.ptrs, X, Y, 0, steps)
-        else:
-            in_b = lib.run_temporal(rule, layout, 64, a.ptrs, b.ptrs, X, Y, 0, steps, k, tile_rows)
-    finally:
-        lib.set_temporal_variant(0)
+    if mode == "simple":
+        in_b = lib.run_simple(rule, layout, 64, a.ptrs, b.ptrs, X, Y, 0, steps, simple_kernel=simple_kernel)
+    else:
+        in_b = lib.run_temporal(rule, layout, 64, a.ptrs, b.ptrs, X, Y, 0, steps, k, tile_rows, row_loop=loop,
+                                words_per_lane=width)
     res = b if in_b else a
     other = a if in_b else b
     del other
@@ -68,11 +66,7 @@ def test_config2_size_temporal_equals_single_step(cuda, rule, k, th, loop, width
     r = lib.rule_id(rule)
     S, steps = 16384, 48
     ref = run(r, 1, S, S, steps, 42, "simple")
-    lib.set_temporal_width(width)
-    try:
-        got = run(r, 1, S, S, steps, 42, "temporal", k, th, loop)
-    finally:
-        lib.set_temporal_width(0)
+    got = run(r, 1, S, S, steps, 42, "temporal", k, th, loop, width)
     assert diff(inputs.PLANES[r], ref, got) == 0
     assert checksum(r, 1, ref, S, S) == checksum(r, 1, got, S, S)
     del ref, got
@@ -95,13 +89,16 @@ def test_config2_size_layouts_agree_on_checksums(cuda):
 
 @pytest.mark.parametrize("rule", ["cyclic", "fluid"])
 def test_config3_size_temporal_equals_single_step(cuda, rule):
+    """Every depth the config-3 workload lets the autotuner choose (k <= 32) at
+    the library's default tile height and both row loops, plus the k = 1
+    single-step candidate, against the single-step kernel on 32768^2."""
     import torch
     r = lib.rule_id(rule)
-    S, steps = 32768, 24
+    S, steps = 32768, 64
     ref = run(r, 0, S, S, steps, 42, "simple")
-    for k, th, loop in ((8, 0, 2), (1, 128, 1)):
+    for k, th, loop in ((16, 0, 2), (16, 0, 1), (24, 0, 2), (32, 0, 2), (12, 0, 2), (8, 0, 2), (1, 128, 1)):
         got = run(r, 0, S, S, steps, 42, "temporal", k, th, loop)
-        assert diff(inputs.PLANES[r], ref, got) == 0, (rule, k)
+        assert diff(inputs.PLANES[r], ref, got) == 0, (rule, k, th, loop)
         del got
         torch.cuda.empty_cache()
     del ref

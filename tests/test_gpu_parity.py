@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 LAYOUTS = [(0, 32), (0, 64), (1, 32), (1, 64)]
 
 
-def run_gpu(oracle, rule, layout, W, cells, steps, mode="simple", k=1, t0=0, tile_rows=0):
+def run_gpu(oracle, rule, layout, W, cells, steps, mode="simple", k=1, t0=0, tile_rows=0, row_loop=0,
+            words_per_lane=0, simple_kernel=0):
     import torch
     from cellato_b200.device import DevicePlanes
     Y, X = cells.shape
@@ -24,9 +25,10 @@ def run_gpu(oracle, rule, layout, W, cells, steps, mode="simple", k=1, t0=0, til
     b = DevicePlanes(nb, X, Y)
     a.upload(oracle.pack(layout, W, nb, cells))
     if mode == "simple":
-        in_b = lib.run_simple(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps)
+        in_b = lib.run_simple(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps, simple_kernel=simple_kernel)
     else:
-        in_b = lib.run_temporal(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps, k, tile_rows)
+        in_b = lib.run_temporal(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps, k, tile_rows,
+                                row_loop=row_loop, words_per_lane=words_per_lane)
     torch.cuda.synchronize()
     res = (b if in_b else a).download()
     return oracle.unpack(layout, W, nb, res, X, Y)
@@ -40,7 +42,7 @@ def test_simple_small_golden(cuda, oracle, golden_small, layout, W):
         assert np.array_equal(out, cout), (case["key"], case["rule"], int((out != cout).sum()))
 
 
-@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 8, 16])
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 8, 16, 24, 32])
 @pytest.mark.parametrize("layout,W", LAYOUTS)
 def test_temporal_small_golden(cuda, oracle, golden_small, layout, W, k):
     for case, cin, cout in golden_small:
@@ -51,21 +53,18 @@ def test_temporal_small_golden(cuda, oracle, golden_small, layout, W, k):
 
 @pytest.mark.parametrize("width", [1, 2])
 @pytest.mark.parametrize("loop", [1, 2])
-@pytest.mark.parametrize("k", [3, 8])
+@pytest.mark.parametrize("k", [3, 8, 24, 32])
 @pytest.mark.parametrize("layout,W", LAYOUTS)
 def test_temporal_row_loops(cuda, oracle, golden_small, layout, W, k, loop, width):
-    """Both row loops (cellato_set_temporal_variant) and both tile widths
-    (cellato_set_temporal_width) of the temporal kernel."""
-    lib.set_temporal_variant(loop)
-    lib.set_temporal_width(width)
-    try:
-        for case, cin, cout in golden_small:
-            r = RULES.index(case["rule"])
-            out = run_gpu(oracle, r, layout, W, cin, case["steps"], mode="temporal", k=k, tile_rows=48)
-            assert np.array_equal(out, cout), (case["key"], case["rule"], k, loop, width)
-    finally:
-        lib.set_temporal_variant(0)
-        lib.set_temporal_width(0)
+    """Both row loops (cellato_tune.row_loop) and both tile widths
+    (cellato_tune.words_per_lane) of the temporal kernel."""
+    # the shortest tile that leaves 16 interior rows below the two k-row halos
+    th = max(48, 2 * ((k + 7) // 8 * 8) + 16)
+    for case, cin, cout in golden_small:
+        r = RULES.index(case["rule"])
+        out = run_gpu(oracle, r, layout, W, cin, case["steps"], mode="temporal", k=k, tile_rows=th, row_loop=loop,
+                      words_per_lane=width)
+        assert np.array_equal(out, cout), (case["key"], case["rule"], k, loop, width)
 
 
 @pytest.mark.parametrize("mode,k", [("simple", 1), ("temporal", 3), ("temporal", 8)])
@@ -149,6 +148,6 @@ def test_streaming_kernel_shapes_and_no_wait_timeouts(cuda, oracle):
             cells = rng.integers(0, inputs.STATES[r], size=(Y, X), dtype=np.uint8)
             want = oracle.run(r, cells, 5, t0=3)
             for W in (32, 64):
-                got = run_gpu(oracle, r, 0, W, cells, 5, t0=3)
+                got = run_gpu(oracle, r, 0, W, cells, 5, t0=3, simple_kernel=2)
                 assert np.array_equal(got, want), (RULES[r], X, Y, W)
     assert lib.device_wait_timeouts() == 0

@@ -10,7 +10,8 @@ import pytest
 
 from conftest import PKG, ROOT, RULES
 
-REF_SRC = "/root/reference/src"
+# the reference tree (its src/ holds the automaton headers); override with CELLATO_REFERENCE_DIR
+REF_SRC = os.path.join(os.environ.get("CELLATO_REFERENCE_DIR", "/root/reference"), "src")
 SRC = os.path.join(ROOT, "tests", "cpp", "source_compat.cpp")
 
 pytestmark = pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference source tree not present")
