@@ -1,8 +1,8 @@
 #ifndef WIRE_CONFIG_HPP
 #define WIRE_CONFIG_HPP
 
-#include "../common_init.hpp"
 #include "./algorithm.hpp"
+#include "./circuit_init.hpp"
 #include "memory/state_dictionary.hpp"
 
 namespace wire {
@@ -16,14 +16,11 @@ struct config {
                                                                       cell_state::electron_tail, cell_state::conductor>;
 
     struct input {
-        // i.i.d. empty/conductor/head/tail = .50/.40/.05/.05, seeded by --seed
+        // the reference's seeded circuit (loops, runs, circles, crossings and
+        // electrons), seeded by --seed
         struct random {
             static std::vector<cell_state> init(cellato::run::run_params& params) {
-                return cellato::automata::iid_grid<cell_state>(
-                    params,
-                    {{cell_state::empty, 0.50}, {cell_state::conductor, 0.40}, {cell_state::electron_head, 0.05},
-                     {cell_state::electron_tail, 0.05}},
-                    params.seed);
+                return circuit_grid<cell_state>(params);
             }
         };
     };

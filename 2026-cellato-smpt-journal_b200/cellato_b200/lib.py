@@ -186,7 +186,8 @@ def tune(simple_kernel: int = 0, row_loop: int = 0, words_per_lane: int = 0, til
 def run_simple(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,
                stream: int = 0, simple_kernel: int = 0) -> int:
     """Returns 1 when the result ended in planes_b, else 0.  simple_kernel as
-    cellato_tune (0 automatic, 1 register bands, 2 bulk-copy streaming)."""
+    cellato_tune (0 automatic, 1 register bands, 2 bulk-copy streaming, 3
+    TMA-fed shared-memory tiles)."""
     out = ctypes.c_int(0)
     t = tune(simple_kernel=simple_kernel)
     check(load().cellato_run_simple(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),

@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "b200/engine.cuh"
+#include "b200/tma_step.cuh"
 
 // Version of the rule_ops layout; cellato_rule_register refuses a table built
 // against another version.
@@ -28,7 +29,7 @@
 
 namespace cellato::b200 {
 // Single-step kernel choices (cellato_tune::simple_kernel).
-enum : int { SIMPLE_AUTO = 0, SIMPLE_REGISTER = 1, SIMPLE_STREAM = 2 };
+enum : int { SIMPLE_AUTO = 0, SIMPLE_REGISTER = 1, SIMPLE_STREAM = 2, SIMPLE_TMA = 3 };
 // Temporal row loops (cellato_tune::row_loop).
 enum : int { LOOP_AUTO = 0, LOOP_ROW_BY_ROW = 1, LOOP_HOISTED = 2 };
 }  // namespace cellato::b200
@@ -136,6 +137,39 @@ struct rule_kernels {
         return cudaGetLastError();
     }
 
+    // the TMA-fed single-step kernel (rows of TMA_SW-word multiples)
+    template <int LAYOUT>
+    static cudaError_t simple_tma(const plane_set& in, const plane_set& out, int Xw, int Y, int t, cudaStream_t s) {
+        using SM = tma_smem<NB, LAYOUT>;
+        const int M = Y / band_rows<LAYOUT>();
+        tma_maps maps;
+        cudaError_t e = make_tma_maps<NB, LAYOUT>(in, Xw, M, maps);
+        if (e != cudaSuccess) return e;
+        auto kern = (t & 1) ? tma_step_kernel<net, NB, LAYOUT, 1> : tma_step_kernel<net, NB, LAYOUT, 0>;
+        const int threads = (TMA_WARPS + 1) * 32;
+        if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::bytes)) !=
+            cudaSuccess)
+            return e;
+        static int sms = 0, per_sm = 0;  // per instantiation; constant for the process's device
+        if (!sms) {
+            int dev = 0, n = 0, b = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+                (e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+                (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, threads, SM::bytes)) != cudaSuccess)
+                return e;
+            per_sm = std::max(1, b);
+            sms = n;
+        }
+        // about two waves of resident CTAs, each range a multiple of a stage
+        const int strips = Xw / TMA_SW;
+        const long long target = 2LL * per_sm * sms;
+        int rows = (int)std::max<long long>(1, ((long long)M * strips + target - 1) / target);
+        rows = (rows + SM::BR - 1) / SM::BR * SM::BR;
+        const dim3 grid(strips, (M + rows - 1) / rows);
+        kern<<<grid, threads, SM::bytes, s>>>(maps, in, out, Xw, M, rows);
+        return cudaGetLastError();
+    }
+
     static cudaError_t take_wait_timeouts(unsigned* count) {
         unsigned zero = 0;
         cudaError_t e = cudaMemcpyFromSymbol(count, g_wait_timeouts, sizeof(unsigned));
@@ -146,6 +180,8 @@ struct rule_kernels {
     template <int LAYOUT>
     static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t, int variant,
                                      cudaStream_t s) {
+        if (variant == SIMPLE_TMA && Xw % TMA_SW == 0 && Y / band_rows<LAYOUT>() >= tma_band<NB, LAYOUT>())
+            return simple_tma<LAYOUT>(in, out, Xw, Y, t, s);
         if constexpr (LAYOUT == LAYOUT_LINEAR) {
             const bool stream_ok = Xw % 4 == 0;
             // default: streaming for rules with two or more planes, whose

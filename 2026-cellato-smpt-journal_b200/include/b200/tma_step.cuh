@@ -1,0 +1,394 @@
+// Single-step kernel fed by the tensor memory accelerator (TMA): one time step
+// per launch, the grid streamed through shared-memory tiles with halos.
+//
+// Work split.  A CTA owns a strip of TMA_SW = 128 linear words (4096 cells per
+// row) and a range of memory rows [m0, m1): a memory row is one row of the
+// linear layout, or one tile row of the tiled layouts (R = 4 or 8 cell rows).
+// Four consumer warps each own 32 words of the strip -- one linear word per
+// lane -- and walk the range top to bottom with a rolling window of three cell
+// rows' features in registers; a fifth warp is the producer.
+//
+// Staging.  A ring of TMA_STAGES shared-memory stages, each BR memory rows of
+// every plane:
+//   * the strip itself: one cp.async.bulk.tensor box per plane and stage
+//     (2-D for the linear layout, 3-D {4 tiles, words, rows} for the tiled
+//     ones), completing on the stage's "full" mbarrier with expect_tx;
+//   * the word to the left and to the right of the strip in each of those rows
+//     (wrapped on the torus): cp.async by the producer's 32 lanes, completing
+//     on the same barrier (cp.async.mbarrier.arrive.noinc);
+//   * the memory row above m0 and below m1 (wrapped) with their halo words:
+//     cp.async into an area of their own, on the "edge" barrier.
+// Consumers arrive on the stage's "empty" barrier once they have read it, and
+// the producer refills it.  No box is ever loaded from another GPU's memory
+// and none uses multicast.
+//
+// Shapes: Xw (linear words per row) a multiple of TMA_SW and at least BR memory
+// rows.  Every global word the kernel touches is inside the planes: rows and
+// words wrap by index, boxes start inside the grid, and the last box of a range
+// may run past the grid's last row, where the TMA writes zeros that are never
+// read.
+//
+// Every wait is bounded.  A consumer whose wait gives up counts it in
+// g_wait_timeouts and leaves; the producer, whose copies write this CTA's
+// shared memory, waits (bounded) for everything it issued before it leaves.
+#ifndef CELLATO_B200_TMA_STEP_CUH
+#define CELLATO_B200_TMA_STEP_CUH
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include "b200/engine.cuh"
+
+namespace cellato::b200 {
+
+constexpr int TMA_WARPS = 4;                // consumer warps
+constexpr int TMA_SW = 32 * TMA_WARPS;      // strip width in linear words
+constexpr int TMA_STAGES = 4;
+constexpr unsigned TMA_WAIT_LIMIT = 1u << 22;
+constexpr int TMA_STAGE_BUDGET = 12 * 1024;  // bytes of strip data per stage (all planes)
+
+// 32-bit words per linear word in one memory row.
+template <int LAYOUT>
+constexpr int tma_lin_words() {
+    return LAYOUT == LAYOUT_LINEAR ? 1 : (LAYOUT == LAYOUT_TILED4 ? 4 : 8);
+}
+
+// Memory rows per stage.
+template <int NB, int LAYOUT>
+constexpr int tma_band() {
+    constexpr int row_bytes = NB * TMA_SW * tma_lin_words<LAYOUT>() * 4;
+    constexpr int b = TMA_STAGE_BUDGET / row_bytes;
+    return b < 1 ? 1 : (b > 32 ? 32 : b);
+}
+
+template <int NB, int LAYOUT>
+struct tma_smem {
+    static constexpr int L = tma_lin_words<LAYOUT>();
+    static constexpr int BR = tma_band<NB, LAYOUT>();
+    static constexpr int plane_block = BR * TMA_SW * L;   // u32 of one plane in one stage
+    static constexpr int ring = TMA_STAGES * NB * plane_block;
+    static constexpr int halo = TMA_STAGES * NB * BR * 2 * L;
+    static constexpr int edge_row = (TMA_SW + 2) * L;       // [left halo][strip][right halo]
+    static constexpr int edge = NB * 2 * edge_row;
+    static constexpr int words = ring + halo + edge;
+    static constexpr size_t bytes = (size_t)words * 4 + (2 * TMA_STAGES + 1) * 8;
+};
+
+struct tma_maps {
+    CUtensorMap m[MAX_PLANES];
+};
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool tma_wait(unsigned long long* bar, unsigned parity) {
+    for (unsigned it = 0; it < TMA_WAIT_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"(BYTES)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Copies linear word gx of memory row m of every plane (L u32 each) to dst
+// (stride `stride` u32 between planes) with cp.async.
+template <int NB, int L>
+__device__ __forceinline__ void copy_word(const plane_set& in, int Xw, int m, int gx, unsigned* dst, int stride) {
+#pragma unroll
+    for (int p = 0; p < NB; ++p) {
+        const word* src = in.p[p] + ((size_t)m * Xw + gx) * L;
+        if constexpr (L == 1) {
+            cp_async<4>(dst + p * stride, src);
+        } else {
+#pragma unroll
+            for (int q = 0; q < L; q += 4) cp_async<16>(dst + p * stride + q, src + q);
+        }
+    }
+}
+
+// The R cell-row words of one linear word at s (L u32 in shared memory).
+template <int LAYOUT>
+__device__ __forceinline__ void rows_of(const unsigned* s, word (&r)[band_rows<LAYOUT>()]) {
+    if constexpr (LAYOUT == LAYOUT_LINEAR) {
+        r[0] = s[0];
+    } else if constexpr (LAYOUT == LAYOUT_TILED4) {
+        const uint4 t = *reinterpret_cast<const uint4*>(s);
+        word a = t.x, b = t.y, c = t.z, d = t.w;
+        transpose4x4(a, b, c, d);
+        r[0] = a, r[1] = b, r[2] = c, r[3] = d;
+    } else {
+        const uint4 t01 = *reinterpret_cast<const uint4*>(s), t23 = *reinterpret_cast<const uint4*>(s + 4);
+        word l0 = t01.x, l1 = t01.z, l2 = t23.x, l3 = t23.z;
+        word h0 = t01.y, h1 = t01.w, h2 = t23.y, h3 = t23.w;
+        transpose4x4(l0, l1, l2, l3);
+        transpose4x4(h0, h1, h2, h3);
+        r[0] = l0, r[1] = l1, r[2] = l2, r[3] = l3, r[4] = h0, r[5] = h1, r[6] = h2, r[7] = h3;
+    }
+}
+
+template <class Net, int NB, int LAYOUT, int TP>
+__global__ void __launch_bounds__((TMA_WARPS + 1) * 32) tma_step_kernel(const __grid_constant__ tma_maps maps,
+                                                                        plane_set in, plane_set out, int Xw, int M,
+                                                                        int rows_per_cta) {
+    using S = tma_smem<NB, LAYOUT>;
+    constexpr int L = S::L, BR = S::BR, R = band_rows<LAYOUT>();
+    using feat = typename Net::feat;
+    extern __shared__ __align__(1024) unsigned tma_sm[];
+    unsigned* ring = tma_sm;
+    unsigned* halo = tma_sm + S::ring;
+    unsigned* edge = halo + S::halo;
+    auto* full = reinterpret_cast<unsigned long long*>(tma_sm + S::words);
+    unsigned long long* empty = full + TMA_STAGES;
+    unsigned long long* edge_bar = empty + TMA_STAGES;
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x0 = blockIdx.x * TMA_SW;
+    const int m0 = blockIdx.y * rows_per_cta;
+    const int m1 = min(M, m0 + rows_per_cta);
+    const int nchunks = (m1 - m0 + BR - 1) / BR;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TMA_STAGES; ++s) {
+            mbar_init(&full[s], 1 + 32);     // the producer's expect_tx arrival + its 32 lanes' cp.async
+            mbar_init(&empty[s], TMA_WARPS);
+        }
+        mbar_init(edge_bar, 32);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (m0 >= m1) return;
+
+    if (warp == TMA_WARPS) {
+        // ---------------- producer
+        const int xl = (x0 + Xw - 1) % Xw, xr = (x0 + TMA_SW) % Xw;
+        // the rows above and below the range, with their halo words
+        for (int e = 0; e < 2; ++e) {
+            const int m = e == 0 ? (m0 + M - 1) % M : m1 % M;
+            unsigned* row = edge + e * S::edge_row;
+            for (int j = lane; j < TMA_SW + 2; j += 32) {
+                const int gx = j == 0 ? xl : (j == TMA_SW + 1 ? xr : x0 + j - 1);
+                copy_word<NB, L>(in, Xw, m, gx, row + j * L, 2 * S::edge_row);
+            }
+        }
+        cp_async_arrive_noinc(edge_bar);
+        bool ok = true;
+        int issued = 0;
+        for (int c = 0; c < nchunks; ++c) {
+            const int s = c % TMA_STAGES;
+            if (c >= TMA_STAGES && !tma_wait(&empty[s], (unsigned)(c / TMA_STAGES - 1) & 1u)) {
+                ok = false;
+                break;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            const int mr = m0 + c * BR;
+            if (lane == 0) {
+                mbar_expect_tx(&full[s], (unsigned)(NB * S::plane_block * 4));
+#pragma unroll
+                for (int p = 0; p < NB; ++p) {
+                    unsigned* dst = ring + (s * NB + p) * S::plane_block;
+                    if constexpr (LAYOUT == LAYOUT_LINEAR)
+                        tma_load_2d(dst, &maps.m[p], x0, mr, &full[s]);
+                    else
+                        tma_load_3d(dst, &maps.m[p], 0, x0, mr, &full[s]);
+                }
+            }
+            // halo words: lane -> (row, side); rows past the range are not needed
+            for (int j = lane; j < 2 * BR; j += 32) {
+                const int r = j >> 1, side = j & 1;
+                if (mr + r < m1)
+                    copy_word<NB, L>(in, Xw, mr + r, side ? xr : xl,
+                                     halo + ((s * NB) * BR + r) * 2 * L + side * L, BR * 2 * L);
+            }
+            cp_async_arrive_noinc(&full[s]);
+            issued = c + 1;
+        }
+        if (!ok && lane == 0) atomicAdd(&g_wait_timeouts, 1u);
+        // every copy this warp issued lands before the CTA's shared memory is released
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        for (int c = max(0, issued - TMA_STAGES); c < issued; ++c)
+            tma_wait(&full[c % TMA_STAGES], (unsigned)(c / TMA_STAGES) & 1u);
+        return;
+    }
+
+    // ---------------- consumers: lane owns linear word x0 + warp*32 + lane
+    const int gx = x0 + warp * 32 + lane;
+    const bool use_l = lane == 0, use_r = lane == 31;
+    // one memory row: R cell rows of this lane's word and of the edge words
+    auto load_row = [&](const unsigned* strip, int strip_stride, const unsigned* lh, const unsigned* rh,
+                        int halo_stride, word (&C)[R][NB], word (&Lw)[R][NB], word (&Rw)[R][NB]) {
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            const unsigned* sp = strip + p * strip_stride;
+            word t[R];
+            rows_of<LAYOUT>(sp + (warp * 32 + lane) * L, t);
+#pragma unroll
+            for (int i = 0; i < R; ++i) C[i][p] = t[i];
+            if (use_l) {
+                rows_of<LAYOUT>(warp > 0 ? sp + (warp * 32 - 1) * L : lh + p * halo_stride, t);
+#pragma unroll
+                for (int i = 0; i < R; ++i) Lw[i][p] = t[i];
+            }
+            if (use_r) {
+                rows_of<LAYOUT>(warp < TMA_WARPS - 1 ? sp + (warp * 32 + 32) * L : rh + p * halo_stride, t);
+#pragma unroll
+                for (int i = 0; i < R; ++i) Rw[i][p] = t[i];
+            }
+        }
+    };
+    auto feats_of = [&](const word (&C)[NB], const word (&Lw)[NB], const word (&Rw)[NB], feat& f) {
+        word CC[NB][1];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) CC[p][0] = C[p];
+        feat fv[1];
+        row_feats<Net, NB, 1>(CC, Lw, Rw, use_l, use_r, fv);
+        f = fv[0];
+    };
+
+    // Rolling window: up / mid / dn are the features of three consecutive cell
+    // rows; the output row is mid's.  Output row i-1 of a memory row is made
+    // while its input row i is read, so res holds a memory row's outputs with
+    // compile-time row indices and is stored once its last row is made (when
+    // the next memory row's first row is read).
+    feat up, mid, dn;
+    word res[R][NB];
+    auto emit = [&](int y, int i) {  // output cell row y into res[i]
+        word o[NB];
+        Net::template eval<TP>(up, mid, dn, y & 1, o);
+#pragma unroll
+        for (int p = 0; p < NB; ++p) res[i][p] = o[p];
+        up = mid;
+        mid = dn;
+    };
+    auto store = [&](int m) {  // the R output rows of memory row m
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+            word rr[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) rr[q] = res[q][p];
+            store_word_rows<LAYOUT>(out.p[p], Xw, m, gx, rr);
+        }
+    };
+    if (!tma_wait(edge_bar, 0)) {
+        if (lane == 0) atomicAdd(&g_wait_timeouts, 1u);
+        return;
+    }
+    {
+        word C[R][NB], Lw[R][NB] = {}, Rw[R][NB] = {};
+        const unsigned* row = edge;  // the row above the range: its last cell row
+        load_row(row + L, 2 * S::edge_row, row, row + (TMA_SW + 1) * L, 2 * S::edge_row, C, Lw, Rw);
+        feats_of(C[R - 1], Lw[R - 1], Rw[R - 1], up);
+    }
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c % TMA_STAGES;
+        if (!tma_wait(&full[s], (unsigned)(c / TMA_STAGES) & 1u)) {
+            if (lane == 0) atomicAdd(&g_wait_timeouts, 1u);
+            return;
+        }
+        const int mr = m0 + c * BR;
+        for (int r = 0; r < BR && mr + r < m1; ++r) {
+            const int m = mr + r;
+            word C[R][NB], Lw[R][NB] = {}, Rw[R][NB] = {};
+            const unsigned* h = halo + ((s * NB) * BR + r) * 2 * L;
+            load_row(ring + (s * NB) * S::plane_block + r * TMA_SW * L, S::plane_block, h, h + L, BR * 2 * L, C, Lw,
+                     Rw);
+            if (m == m0) {
+                feats_of(C[0], Lw[0], Rw[0], mid);
+            } else {
+                feats_of(C[0], Lw[0], Rw[0], dn);
+                emit(m * R - 1, R - 1);
+                store(m - 1);
+            }
+#pragma unroll
+            for (int i = 1; i < R; ++i) {
+                feats_of(C[i], Lw[i], Rw[i], dn);
+                emit(m * R + i - 1, i - 1);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    {
+        word C[R][NB], Lw[R][NB] = {}, Rw[R][NB] = {};
+        const unsigned* row = edge + S::edge_row;  // the row below the range: its first cell row
+        load_row(row + L, 2 * S::edge_row, row, row + (TMA_SW + 1) * L, 2 * S::edge_row, C, Lw, Rw);
+        feats_of(C[0], Lw[0], Rw[0], dn);
+        emit(m1 * R - 1, R - 1);
+        store(m1 - 1);
+    }
+}
+
+// ---------------------------------------------------------------- host side
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// Tensor maps of nb planes for the TMA step kernel: linear planes as 2-D
+// {Xw words, M rows} of u32, tiled planes as 3-D {4 tiles, Xw linear words, M
+// tile rows} of u32 (4-row tiles) or u64 (8-row tiles); boxes of one stage.
+template <int NB, int LAYOUT>
+inline cudaError_t make_tma_maps(const plane_set& ps, int Xw, int M, tma_maps& maps) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    constexpr int BR = tma_band<NB, LAYOUT>();
+    for (int p = 0; p < NB; ++p) {
+        CUresult r;
+        if constexpr (LAYOUT == LAYOUT_LINEAR) {
+            const cuuint64_t dims[2] = {(cuuint64_t)Xw, (cuuint64_t)M};
+            const cuuint64_t strides[1] = {(cuuint64_t)Xw * 4};
+            const cuuint32_t box[2] = {TMA_SW, BR};
+            const cuuint32_t es[2] = {1, 1};
+            r = enc(&maps.m[p], CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, ps.p[p], dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        } else {
+            constexpr bool t8 = LAYOUT == LAYOUT_TILED8;
+            const cuuint64_t esz = t8 ? 8 : 4;
+            const cuuint64_t dims[3] = {4, (cuuint64_t)Xw, (cuuint64_t)M};
+            const cuuint64_t strides[2] = {4 * esz, (cuuint64_t)Xw * 4 * esz};
+            const cuuint32_t box[3] = {4, TMA_SW, BR};
+            const cuuint32_t es[3] = {1, 1, 1};
+            r = enc(&maps.m[p], t8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, ps.p[p], dims,
+                    strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        }
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace cellato::b200
+
+#endif  // CELLATO_B200_TMA_STEP_CUH

@@ -53,6 +53,10 @@ SIZE = 16384
 CA_STEPS = 1000
 LAYOUT = 1        # tiled_bit_planes
 WORD_BITS = 64
+# word sizes the autotuner may pick per layout: the tiled layout's tile shape
+# depends on it (8 x 4 or 8 x 8 cells); linear words of 32 and 64 bits are the
+# same bytes and the same kernels, so the linear workload keeps 64
+WORD_CHOICES = {0: (64,), 1: (32, 64)}
 SEED = 42
 BATCH_CANDIDATES = (("temporal", 2), ("temporal", 4), ("temporal", 8), ("temporal", 12), ("temporal", 16))
 CPU_SAMPLE_SIZE = 2048
@@ -73,15 +77,15 @@ MEASURED_TRAFFIC = {
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
 # temporal kernel configuration, from one ncu capture of that configuration
-# (summary in profiles/); keyed by (rule, layout, k, tile_rows, row loop, words
-# per lane, size), tile_rows 0 being the library's default height.  Each
+# (summary in profiles/); keyed by (rule, layout, word size, k, tile_rows, row
+# loop, words per lane, size), tile_rows 0 being the library's default height.  Each
 # configuration is timed live and set against the ALU pipe's measured rate
 # (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 16, 0, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md", None),
-    ("excitable", 1, 16, 0, 2, 1, 16384): (70207344, "profiles/alu_pipe_temporal_kernels.md", None),
-    ("cyclic", 0, 16, 0, 2, 1, 32768): (1664571440, "profiles/alu_pipe_temporal_kernels.md", None),
-    ("fluid", 0, 16, 0, 2, 1, 32768): (312104380, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("wire", 1, 64, 16, 0, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("excitable", 1, 64, 16, 0, 2, 1, 16384): (70207344, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("cyclic", 0, 64, 16, 0, 2, 1, 32768): (1664571440, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("fluid", 0, 64, 16, 0, 2, 1, 32768): (312104380, "profiles/alu_pipe_temporal_kernels.md", None),
 }
 
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
@@ -333,22 +337,25 @@ def parse_choices(text: str) -> dict:
 
 
 def describe_choice(c: dict) -> str:
-    """The autotuner's choice as text: mode, k, tile rows (0 = default) and row loop."""
+    """The autotuner's choice as text: mode, k, tile rows (0 = default), row
+    loop, tile width and, when tuned, the word size."""
+    w = f" W{c['word_bits']}" if "word_bits" in c else ""
     if c["mode"] != "temporal":
-        return c["mode"]
+        return c["mode"] + w
     loop = {0: "default", 1: "row-by-row", 2: "hoisted"}[c.get("loop", 0)]
     width = {0: "default", 1: "1", 2: "2"}[c.get("width", 0)]
-    return f"temporal k={c['k']} tile_rows={c.get('tile_rows', 0)} loop={loop} words_per_lane={width}"
+    return f"temporal k={c['k']} tile_rows={c.get('tile_rows', 0)} loop={loop} words_per_lane={width}{w}"
 
 
 def workload_config(args, extra=None):
     from cellato_b200 import inputs
     layout = "tiled_bit_planes" if LAYOUT == 1 else "bit_planes"
     mib = [2 * inputs.PLANES[inputs.RULE_ID[a]] * args.size * args.size // 8 >> 20 for a in AUTOMATA]
-    c = {"workload": f"{'+'.join(AUTOMATA)} {args.size}x{args.size} {layout} W{WORD_BITS}, {args.ca_steps} steps "
+    words = "W32 or W64 autotuned" if len(WORD_CHOICES[LAYOUT]) > 1 else f"W{WORD_CHOICES[LAYOUT][0]}"
+    c = {"workload": f"{'+'.join(AUTOMATA)} {args.size}x{args.size} {layout} {words}, {args.ca_steps} steps "
                      f"each, traverser autotuned (simple | temporal k <= {K_MAX})",
          "automata": list(AUTOMATA), "x_size": args.size, "y_size": args.size, "ca_steps_per_step": args.ca_steps,
-         "layout": layout, "word_size": WORD_BITS,
+         "layout": layout, "word_size": list(WORD_CHOICES[LAYOUT]),
          "l2": f"inputs larger than L2 (ping-pong planes {' MiB + '.join(str(m) for m in mib)} MiB), no flush"}
     if extra:
         c.update(extra)
@@ -368,27 +375,28 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
     X = Y = args.size
+    # autotune per automaton, unless pinned: the traverser and, for the tiled
+    # layout, whose word size the workload leaves open, the word size (32-bit
+    # words: 8 x 4 tiles, 64-bit words: 8 x 8); then the planes in that layout
+    pinned = parse_choices(args.choice)
+    cands = [c for c in autotune.DEFAULT_CANDIDATES if c[1] <= K_MAX]
     grids = {}
     for a in AUTOMATA:
         r = inputs.RULE_ID[a]
         nb = inputs.PLANES[r]
         cells = torch.from_numpy(inputs.workload_grid(a, X, Y, SEED + rank)).to(dev)
+        if a in pinned:
+            choice = dict(pinned[a], word_bits=WORD_BITS)
+        else:
+            choice = autotune.tune_word_bits(r, LAYOUT, cells, X, Y, word_bits=WORD_CHOICES[LAYOUT],
+                                             candidates=cands, use_cache=False)
+        W = choice["word_bits"]
         pa, pb = DevicePlanes(nb, X, Y, dev), DevicePlanes(nb, X, Y, dev)
-        pa.pack_from(cells, LAYOUT, WORD_BITS, sp)
+        pa.pack_from(cells, LAYOUT, W, sp)
         init = DevicePlanes(nb, X, Y, dev)
         init.buf.copy_(pa.buf)
         del cells
-        grids[a] = {"rule": r, "nb": nb, "a": pa, "b": pb, "init": init}
-    torch.cuda.synchronize()
-
-    # autotune per automaton (on scratch copies of the planes), unless pinned
-    pinned = parse_choices(args.choice)
-    for a, g in grids.items():
-        cands = [c for c in autotune.DEFAULT_CANDIDATES if c[1] <= K_MAX]
-        choice = pinned.get(a) or autotune.tune(g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y,
-                                                candidates=cands, use_cache=False)
-        g["choice"] = choice
-        g["a"].buf.copy_(g["init"].buf)
+        grids[a] = {"rule": r, "nb": nb, "a": pa, "b": pb, "init": init, "choice": choice, "W": W}
     torch.cuda.synchronize()
 
     def launches(g):
@@ -412,7 +420,7 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
                 st.wait_event(fork)
             if events is not None:
                 events[a][0].record(st)
-            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, t0,
+            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, t0,
                                 args.ca_steps, st.cuda_stream)
             if in_b:
                 g["a"], g["b"] = g["b"], g["a"]
@@ -499,7 +507,7 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
             nb, pb_ = g["nb"], g["init"].plane_bytes
             st = stream if args.sequential else comp[a]
             st.wait_event(in_ready[a])
-            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, t0,
+            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, t0,
                                 args.ca_steps, st.cuda_stream)
             computed[a].record(st)
             res = g["b"] if in_b else g["a"]
@@ -530,7 +538,7 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
     e2e_ok = True
     for a, g in grids.items():
         g["a"].buf.copy_(g["init"].buf)
-        in_b = autotune.run(g["choice"], g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0,
+        in_b = autotune.run(g["choice"], g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, 0,
                             args.ca_steps, sp)
         res = g["b"] if in_b else g["a"]
         torch.cuda.synchronize()
@@ -541,13 +549,13 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
     # (one step per launch: read and write every plane once)
     single = {}
     for a, g in grids.items():
-        c1 = autotune.tune(g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y,
+        c1 = autotune.tune(g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y,
                            candidates=autotune.SINGLE_STEP_CANDIDATES, use_cache=False)
         g["a"].buf.copy_(g["init"].buf)
         n1 = 16
-        autotune.run(c1, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, 2, sp)
+        autotune.run(c1, g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, 0, 2, sp)
         e0.record(stream)
-        autotune.run(c1, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, n1, sp)
+        autotune.run(c1, g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, 0, n1, sp)
         e1.record(stream)
         torch.cuda.synchronize()
         ms1 = e0.elapsed_time(e1) / n1
@@ -566,16 +574,16 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
            "peak_source": "measured live: cellato_lop3_rate (independent lop3.b32 chains, full occupancy)",
            "kernels": {}}
     for key in MEASURED_ALU:
-        a, lay, k, th, loop, width, size = key
-        if a not in grids or lay != LAYOUT or size != args.size:
+        a, lay, wb, k, th, loop, width, size = key
+        if a not in grids or lay != LAYOUT or size != args.size or wb != grids[a]["W"]:
             continue
         count, src, fresh = measured(MEASURED_ALU, key, a)
         g = grids[a]
         c = {"mode": "temporal", "k": k, "tile_rows": th, "loop": loop, "width": width}
         nl = 8
-        autotune.run(c, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, 2 * k, sp)
+        autotune.run(c, g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, 0, 2 * k, sp)
         e0.record(stream)
-        autotune.run(c, g["rule"], LAYOUT, WORD_BITS, g["a"].ptrs, g["b"].ptrs, X, Y, 0, nl * k, sp)
+        autotune.run(c, g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, 0, nl * k, sp)
         e1.record(stream)
         torch.cuda.synchronize()
         msl = e0.elapsed_time(e1) / nl
@@ -660,8 +668,7 @@ def batched_arm(args, rank: int, world: int):
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
     rng = np.random.default_rng(SEED + rank)
-    layout, W = LAYOUT, WORD_BITS
-    R = W // 8
+    layout = LAYOUT
     specs = []
     lo, hi = np.log(args.batch_min_side), np.log(args.batch_max_side)
     for _ in range(args.batch_grids):
@@ -671,42 +678,52 @@ def batched_arm(args, rank: int, world: int):
         X, Y = side * np.sqrt(aspect), side / np.sqrt(aspect)
         if rng.integers(0, 2):
             X, Y = Y, X
-        X = max(64, int(round(X / 64)) * 64)          # quantised to the layout: X multiple of 64,
-        Y = max(2 * R, int(round(Y / (2 * R))) * 2 * R)  # Y multiple of 2 tile rows (even for critters)
+        X = max(64, int(round(X / 64)) * 64)   # quantised: X a multiple of 64, Y of 16 (two 8-row tiles,
+        Y = max(16, int(round(Y / 16)) * 16)   # even for critters), so that either word size fits
         steps = int(rng.integers(10, args.batch_max_steps + 1))
         specs.append((rule, X, Y, steps))
-    # device-generated seeded inputs at each automaton's reference density
-    bufs = []
-    g = torch.Generator(device=dev)
-    for i, (rule, X, Y, steps) in enumerate(specs):
-        name = inputs.RULES[rule]
-        probs = inputs.REFERENCE_DENSITY[name]
+    gen = torch.Generator(device=dev)
+
+    def cells_of(i):
+        """Grid i's seeded initial state at its automaton's reference density."""
+        rule, X, Y, _ = specs[i]
+        probs = inputs.REFERENCE_DENSITY[inputs.RULES[rule]]
         vals = torch.tensor(list(probs.keys()), dtype=torch.uint8, device=dev)
         cum = torch.tensor(np.cumsum(list(probs.values())), dtype=torch.float64, device=dev)
-        g.manual_seed(SEED * 100003 + i)
-        u = torch.rand((Y, X), generator=g, device=dev, dtype=torch.float64)
-        k = torch.clamp(torch.bucketize(u, cum), max=len(vals) - 1)
-        cells = vals[k].contiguous()
+        gen.manual_seed(SEED * 100003 + i)
+        u = torch.rand((Y, X), generator=gen, device=dev, dtype=torch.float64)
+        return vals[torch.clamp(torch.bucketize(u, cum), max=len(vals) - 1)].contiguous()
+
+    # the autotuner: temporal depth per automaton on that automaton's median-sized
+    # grid, at each word size; the batch takes the word size with the lower
+    # total time over its cell updates (one word size holds for a whole batch)
+    from cellato_b200 import autotune
+    median = {}
+    for r in sorted({s[0] for s in specs}):
+        mine = sorted((X * Y, i) for i, (rr, X, Y, _) in enumerate(specs) if rr == r)
+        median[r] = mine[len(mine) // 2][1]
+    work = {r: sum(X * Y * s for rr, X, Y, s in specs if rr == r) for r in median}
+    tuned = {}
+    for W in WORD_CHOICES[layout]:
+        for r, i in median.items():
+            _, X, Y, _ = specs[i]
+            sa, sb = DevicePlanes(inputs.PLANES[r], X, Y, dev), DevicePlanes(inputs.PLANES[r], X, Y, dev)
+            sa.pack_from(cells_of(i), layout, W)
+            tuned[(W, r)] = autotune.tune(r, layout, W, sa.ptrs, sb.ptrs, X, Y, candidates=BATCH_CANDIDATES,
+                                          use_cache=False)
+            del sa, sb
+    W = min(WORD_CHOICES[layout], key=lambda w: sum(tuned[(w, r)]["ns_per_cell_step"] * work[r] for r in median))
+    ks = {r: tuned[(W, r)]["k"] for r in median}
+
+    bufs = []
+    for i, (rule, X, Y, steps) in enumerate(specs):
         nb = inputs.PLANES[rule]
         a, b = DevicePlanes(nb, X, Y, dev), DevicePlanes(nb, X, Y, dev)
-        a.pack_from(cells, layout, W)
+        a.pack_from(cells_of(i), layout, W)
         init = DevicePlanes(nb, X, Y, dev)
         init.buf.copy_(a.buf)
         bufs.append((a, b, init))
     torch.cuda.synchronize()
-    # temporal depth per automaton from the autotuner, measured on scratch copies of the
-    # median-sized grid of that automaton in the batch
-    from cellato_b200 import autotune
-    ks = {}
-    for r in sorted({s[0] for s in specs}):
-        mine = sorted((X * Y, i) for i, (rr, X, Y, _) in enumerate(specs) if rr == r)
-        i = mine[len(mine) // 2][1]
-        _, X, Y, _ = specs[i]
-        sa, sb = DevicePlanes(inputs.PLANES[r], X, Y, dev), DevicePlanes(inputs.PLANES[r], X, Y, dev)
-        sa.buf.copy_(bufs[i][0].buf)
-        choice = autotune.tune(r, layout, W, sa.ptrs, sb.ptrs, X, Y, candidates=BATCH_CANDIDATES, use_cache=False)
-        ks[r] = choice["k"]
-        del sa, sb
     cells_total = sum(X * Y * s for _, X, Y, s in specs)
 
     batch = Batch(layout, W, [(r, X, Y, s, a.ptrs, b.ptrs) for (r, X, Y, s), (a, b, _) in zip(specs, bufs)], ks)
@@ -756,8 +773,10 @@ def batched_arm(args, rank: int, world: int):
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded, device-generated at reference densities)",
         "config": {"workload": f"batched: {args.batch_grids} grids, sides log-uniform {args.batch_min_side}-"
                                f"{args.batch_max_side}, aspect 1-4, 10 automata uniform, steps uniform "
-                               f"10-{args.batch_max_steps}; tiled_bit_planes W64, k autotuned per automaton; one CUDA-graph launch",
+                               f"10-{args.batch_max_steps}; tiled_bit_planes, word size and k autotuned; "
+                               f"one CUDA-graph launch",
                    "k_per_automaton": {inputs.RULES[r]: k for r, k in ks.items()},
+                   "word_bits": W,
                    "quantisation": "X to a multiple of 64, Y to a multiple of 16",
                    "cells_updates_per_step": cells_total, "graph_kernel_launches": info["kernel_launches"],
                    "work_items": info["work_items"]},

@@ -89,8 +89,9 @@ typedef struct cellato_rule_ops_st cellato_rule_ops;
  * temporal_tile_size_y); here they select among this library's kernels.  Every
  * choice gives the same results. */
 typedef struct {
-    int simple_kernel;   /* single-step kernel, linear layout: 0 automatic, 1 register bands, 2 bulk-copy
-                            streaming (rows of 16-byte multiples; others use 1) */
+    int simple_kernel;   /* single-step kernel: 0 automatic, 1 register bands, 2 bulk-copy streaming (linear
+                            layout, rows of 16-byte multiples; others use 1), 3 TMA-fed shared-memory tiles
+                            (rows of a multiple of 4096 cells; others use 1) */
     int row_loop;        /* temporal row loop: 0 automatic, 1 row by row, 2 the input rows of each three-row
                             trip read before its in-place writes */
     int words_per_lane;  /* temporal tile width: 0 the rule's default (2 for one-plane rules, else 1), 1, or 2

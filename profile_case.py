@@ -28,7 +28,7 @@ def main() -> None:
     ap.add_argument("--layout", default="tiled_bit_planes", choices=list(lib.LAYOUTS))
     ap.add_argument("--word-bits", type=int, default=64)
     ap.add_argument("--size", type=int, default=16384)
-    ap.add_argument("--mode", default="temporal", choices=["simple", "temporal", "ops", "lop3"],
+    ap.add_argument("--mode", default="temporal", choices=["simple", "temporal", "ops", "lop3", "batch"],
                     help="ops: the whole-grid operations (checksum, diff, random fill, packing, bit_array "
                          "conversion), each run --launches times; lop3: the ALU-pipe rate kernel "
                          "(cellato_lop3_rate: one warm-up and three timed launches)")
@@ -38,6 +38,9 @@ def main() -> None:
     ap.add_argument("--width", type=int, default=0, help="temporal words per lane (cellato_tune.words_per_lane)")
     ap.add_argument("--simple-kernel", type=int, default=0, help="single-step kernel (cellato_tune.simple_kernel)")
     ap.add_argument("--launches", type=int, default=3)
+    ap.add_argument("--grids", type=int, default=512, help="batch: grids in the batch (the batched workload's "
+                                                            "distribution: sides 64-4096, aspect 1-4, 10 automata)")
+    ap.add_argument("--max-steps", type=int, default=1000, help="batch: steps per grid uniform in 10..this")
     ap.add_argument("--warmup", type=int, default=1)
     a = ap.parse_args()
 
@@ -47,6 +50,8 @@ def main() -> None:
         return
     if a.mode == "ops":
         return ops(a, r)
+    if a.mode == "batch":
+        return batch(a)
     nb = lib.rule_planes(r)
     layout = lib.LAYOUTS[a.layout]
     X = Y = a.size
@@ -119,6 +124,46 @@ def ops(a, r) -> None:
         out[name] = {"ms": round(ms, 4), "algorithmic_bytes": byt, "gbs": round(byt / (ms * 1e-3) / 1e9, 1)}
     print(json.dumps({"rule": inputs.RULES[r], "layout": a.layout, "word_bits": a.word_bits, "size": a.size,
                       "ops": out}))
+
+
+def batch(a) -> None:
+    """One batch of the batched workload's distribution (device-seeded, the same
+    k for every rule), launched --launches times after --warmup launches."""
+    import numpy as np
+    from cellato_b200.batch import Batch
+    rng = np.random.default_rng(42)
+    layout, W = lib.LAYOUTS[a.layout], a.word_bits
+    lo, hi = np.log(64), np.log(4096)
+    grids, keep, cells = [], [], 0
+    for i in range(a.grids):
+        rule = int(rng.integers(0, 10))
+        side = float(np.exp(rng.uniform(lo, hi)))
+        aspect = float(rng.uniform(1.0, 4.0))
+        X, Y = side * np.sqrt(aspect), side / np.sqrt(aspect)
+        if rng.integers(0, 2):
+            X, Y = Y, X
+        X, Y = max(64, int(round(X / 64)) * 64), max(16, int(round(Y / 16)) * 16)
+        steps = int(rng.integers(min(10, a.max_steps), a.max_steps + 1))
+        nb = lib.rule_planes(rule)
+        pa, pb = DevicePlanes(nb, X, Y), DevicePlanes(nb, X, Y)
+        lib.fill_random(layout, W, nb, pa.ptrs, X, Y, 1000 + i,
+                        inputs.thresholds(inputs.REFERENCE_DENSITY[inputs.RULES[rule]]))
+        grids.append((rule, X, Y, steps, pa.ptrs, pb.ptrs))
+        keep.append((pa, pb))
+        cells += X * Y * steps
+    b = Batch(layout, W, grids, {r: a.k for r in range(10)})
+    for _ in range(a.warmup):
+        b.launch()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.launches):
+        b.launch()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.launches
+    print(json.dumps({"mode": "batch", "grids": a.grids, "k": a.k, "word_bits": W, "ms_per_launch": round(ms, 3),
+                      "gcups": round(cells / (ms * 1e-3) / 1e9, 1), **b.info()}))
 
 
 if __name__ == "__main__":

@@ -76,3 +76,32 @@ extern "C" int host_lowered_run(int rule, const uint8_t* in, uint8_t* out, int X
     }
     return -1;
 }
+
+// The seeded initial grid of each automaton config (config::input::random,
+// what the cellato CLI starts from), as dictionary indices.
+template <class A>
+int config_init(int X, int Y, int seed, uint8_t* out) {
+    cellato::run::run_params params;
+    params.x_size = X;
+    params.y_size = Y;
+    params.seed = seed;
+    const auto st = A::input::random::init(params);
+    for (std::size_t i = 0; i < st.size(); ++i) out[i] = (uint8_t)A::state_dictionary::state_to_index(st[i]);
+    return 0;
+}
+
+extern "C" int host_config_init(int rule, int X, int Y, int seed, uint8_t* out) {
+    switch (rule) {
+        case 0: return config_init<game_of_life::config>(X, Y, seed, out);
+        case 1: return config_init<fire::config>(X, Y, seed, out);
+        case 2: return config_init<wire::config>(X, Y, seed, out);
+        case 3: return config_init<excitable::config>(X, Y, seed, out);
+        case 4: return config_init<brian::config>(X, Y, seed, out);
+        case 5: return config_init<maze::config>(X, Y, seed, out);
+        case 6: return config_init<cyclic::config>(X, Y, seed, out);
+        case 7: return config_init<fluid::config>(X, Y, seed, out);
+        case 8: return config_init<critters::config>(X, Y, seed, out);
+        case 9: return config_init<traffic::config>(X, Y, seed, out);
+    }
+    return -1;
+}

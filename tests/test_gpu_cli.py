@@ -29,8 +29,6 @@ def test_cli_checksums_match_reference(cuda, traverser, layout, word):
     header = run_cli(["--print_csv_header"]).split(",")
     X, Y, steps, seed = 256, 128, 24, 7
     for rule, name in enumerate(RULES):
-        if name == "wire":
-            continue  # the reference seeds wire with a structured circuit, this library with an i.i.d. mix
         args = ["--automaton", name, "--device", "CUDA", "--traverser", traverser, "--evaluator", layout,
                 "--layout", layout, "--word_size", str(word), "--x_size", str(X), "--y_size", str(Y),
                 "--steps", str(steps), "--seed", str(seed), "--rounds", "2"]
@@ -65,8 +63,6 @@ def test_cli_bit_array_checksums_match_reference(cuda, word, X):
     header = run_cli(["--print_csv_header"]).split(",")
     Y, steps, seed = 40, 17, 11
     for rule, name in enumerate(RULES):
-        if name == "wire":
-            continue
         args = ["--automaton", name, "--device", "CUDA", "--traverser", "simple", "--evaluator", "bit_array",
                 "--layout", "bit_array", "--word_size", str(word), "--x_size", str(X), "--y_size", str(Y),
                 "--steps", str(steps), "--seed", str(seed), "--rounds", "2"]

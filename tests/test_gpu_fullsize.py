@@ -103,3 +103,26 @@ def test_config3_size_temporal_equals_single_step(cuda, rule):
         torch.cuda.empty_cache()
     del ref
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("rule,layout,S,W", [("wire", 1, 16384, 32), ("excitable", 1, 16384, 64),
+                                             ("cyclic", 0, 32768, 64), ("fluid", 0, 32768, 64)])
+def test_tma_single_step_equals_register_kernel(cuda, rule, layout, S, W):
+    """The TMA-fed single-step kernel against the register-band kernel at the
+    workloads' full sizes, both word sizes of the tiled layout."""
+    import torch
+    from cellato_b200.device import DevicePlanes
+    r = lib.rule_id(rule)
+    nb = inputs.PLANES[r]
+    steps = 7
+    outs = []
+    for kernel in (1, 3):
+        a, b = DevicePlanes(nb, S, S), DevicePlanes(nb, S, S)
+        lib.fill_random(layout, W, nb, a.ptrs, S, S, 9, inputs.thresholds(inputs.REFERENCE_DENSITY[rule]))
+        in_b = lib.run_simple(r, layout, W, a.ptrs, b.ptrs, S, S, 0, steps, simple_kernel=kernel)
+        outs.append(b if in_b else a)
+        del a, b
+    assert diff(nb, outs[0], outs[1]) == 0
+    assert lib.device_wait_timeouts() == 0
+    del outs
+    torch.cuda.empty_cache()

@@ -151,3 +151,18 @@ def test_streaming_kernel_shapes_and_no_wait_timeouts(cuda, oracle):
                 got = run_gpu(oracle, r, 0, W, cells, 5, t0=3, simple_kernel=2)
                 assert np.array_equal(got, want), (RULES[r], X, Y, W)
     assert lib.device_wait_timeouts() == 0
+
+
+@pytest.mark.parametrize("layout,W", LAYOUTS)
+def test_tma_single_step_kernel(cuda, oracle, layout, W):
+    """The TMA-fed single-step kernel (cellato_tune.simple_kernel = 3, rows of
+    a multiple of 4096 cells): every rule, one and two strips per row, heights
+    from one stage to several CTAs per strip, wrapped halos, odd step offsets."""
+    rng = np.random.default_rng(31 + layout + W)
+    for r in range(10):
+        for X, Y in [(4096, 96), (8192, 40), (4096, 264)]:
+            cells = rng.integers(0, inputs.STATES[r], size=(Y, X), dtype=np.uint8)
+            want = oracle.run(r, cells, 5, t0=3)
+            got = run_gpu(oracle, r, layout, W, cells, 5, t0=3, simple_kernel=3)
+            assert np.array_equal(got, want), (RULES[r], X, Y, layout, W)
+    assert lib.device_wait_timeouts() == 0
