@@ -137,16 +137,21 @@ struct rule_kernels {
         return cudaGetLastError();
     }
 
-    // the TMA-fed single-step kernel (rows of TMA_SW-word multiples)
+    // the TMA-fed single-step kernel (rows of a multiple of its strip width)
+    static constexpr int TMA_V = tma_default_v<NB>();
+    template <int LAYOUT>
+    static bool tma_fits(int Xw, int Y) {
+        using G = tma_geom<NB, LAYOUT, TMA_V>;
+        return Xw % G::SW == 0 && Y / band_rows<LAYOUT>() >= G::BR;
+    }
     template <int LAYOUT>
     static cudaError_t simple_tma(const plane_set& in, const plane_set& out, int Xw, int Y, int t, cudaStream_t s) {
-        using SM = tma_smem<NB, LAYOUT>;
+        using SM = tma_geom<NB, LAYOUT, TMA_V>;
         const int M = Y / band_rows<LAYOUT>();
         tma_maps maps;
-        cudaError_t e = make_tma_maps<NB, LAYOUT>(in, Xw, M, maps);
+        cudaError_t e = make_tma_maps<NB, LAYOUT, TMA_V>(in, Xw, M, maps);
         if (e != cudaSuccess) return e;
-        auto kern = (t & 1) ? tma_step_kernel<net, NB, LAYOUT, 1> : tma_step_kernel<net, NB, LAYOUT, 0>;
-        const int threads = (TMA_WARPS + 1) * 32;
+        auto kern = (t & 1) ? tma_step_kernel<net, NB, LAYOUT, TMA_V, 1> : tma_step_kernel<net, NB, LAYOUT, TMA_V, 0>;
         if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::bytes)) !=
             cudaSuccess)
             return e;
@@ -155,18 +160,18 @@ struct rule_kernels {
             int dev = 0, n = 0, b = 0;
             if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
                 (e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-                (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, threads, SM::bytes)) != cudaSuccess)
+                (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, SM::threads, SM::bytes)) != cudaSuccess)
                 return e;
             per_sm = std::max(1, b);
             sms = n;
         }
-        // about two waves of resident CTAs, each range a multiple of a stage
-        const int strips = Xw / TMA_SW;
-        const long long target = 2LL * per_sm * sms;
+        // one wave of resident CTAs with equal ranges (a multiple of a stage)
+        const int strips = Xw / SM::SW;
+        const long long target = (long long)per_sm * sms;
         int rows = (int)std::max<long long>(1, ((long long)M * strips + target - 1) / target);
         rows = (rows + SM::BR - 1) / SM::BR * SM::BR;
         const dim3 grid(strips, (M + rows - 1) / rows);
-        kern<<<grid, threads, SM::bytes, s>>>(maps, in, out, Xw, M, rows);
+        kern<<<grid, SM::threads, SM::bytes, s>>>(maps, in, out, Xw, M, rows);
         return cudaGetLastError();
     }
 
@@ -180,8 +185,7 @@ struct rule_kernels {
     template <int LAYOUT>
     static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t, int variant,
                                      cudaStream_t s) {
-        if (variant == SIMPLE_TMA && Xw % TMA_SW == 0 && Y / band_rows<LAYOUT>() >= tma_band<NB, LAYOUT>())
-            return simple_tma<LAYOUT>(in, out, Xw, Y, t, s);
+        if (variant == SIMPLE_TMA && tma_fits<LAYOUT>(Xw, Y)) return simple_tma<LAYOUT>(in, out, Xw, Y, t, s);
         if constexpr (LAYOUT == LAYOUT_LINEAR) {
             const bool stream_ok = Xw % 4 == 0;
             // default: streaming for rules with two or more planes, whose
