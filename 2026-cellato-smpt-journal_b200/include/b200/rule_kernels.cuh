@@ -138,20 +138,22 @@ struct rule_kernels {
     }
 
     // the TMA-fed single-step kernel (rows of a multiple of its strip width)
-    static constexpr int TMA_V = tma_default_v<NB>();
+    template <int LAYOUT>
+    static constexpr int TMA_V = tma_default_v<NB, LAYOUT>();
     template <int LAYOUT>
     static bool tma_fits(int Xw, int Y) {
-        using G = tma_geom<NB, LAYOUT, TMA_V>;
+        using G = tma_geom<NB, LAYOUT, TMA_V<LAYOUT>>;
         return Xw % G::SW == 0 && Y / band_rows<LAYOUT>() >= G::BR;
     }
     template <int LAYOUT>
     static cudaError_t simple_tma(const plane_set& in, const plane_set& out, int Xw, int Y, int t, cudaStream_t s) {
-        using SM = tma_geom<NB, LAYOUT, TMA_V>;
+        constexpr int V = TMA_V<LAYOUT>;
+        using SM = tma_geom<NB, LAYOUT, V>;
         const int M = Y / band_rows<LAYOUT>();
         tma_maps maps;
-        cudaError_t e = make_tma_maps<NB, LAYOUT, TMA_V>(in, Xw, M, maps);
+        cudaError_t e = make_tma_maps<NB, LAYOUT, V>(in, Xw, M, maps);
         if (e != cudaSuccess) return e;
-        auto kern = (t & 1) ? tma_step_kernel<net, NB, LAYOUT, TMA_V, 1> : tma_step_kernel<net, NB, LAYOUT, TMA_V, 0>;
+        auto kern = (t & 1) ? tma_step_kernel<net, NB, LAYOUT, V, 1> : tma_step_kernel<net, NB, LAYOUT, V, 0>;
         if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::bytes)) !=
             cudaSuccess)
             return e;

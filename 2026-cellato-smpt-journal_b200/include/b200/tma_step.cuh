@@ -4,9 +4,8 @@
 // Work split.  A CTA owns a strip of SW linear words and a range of memory
 // rows [m0, m1): a memory row is one row of the linear layout, or one tile row
 // of the tiled layouts (R = 4 or 8 cell rows).  Each consumer warp owns 32 x V
-// consecutive words of the strip -- V per lane, 4 for one-plane rules, 2 for
-// two or three planes, else 1, so that lane shuffles and per-word overheads
-// are shared by V words -- and walks the range top to bottom with a rolling
+// consecutive words of the strip -- V per lane (tma_default_v), so that lane
+// shuffles and per-word overheads are shared by V words -- and walks the range top to bottom with a rolling
 // window of three cell rows' features in registers, loading and featurising a
 // group of rows at a time (a tile row's R rows, or up to four linear rows) so
 // that independent work overlaps.  SW = 32 x V x consumer warps is 128 words
@@ -52,10 +51,15 @@ constexpr int TMA_STAGES = 3;
 constexpr unsigned TMA_WAIT_LIMIT = 1u << 22;
 constexpr int TMA_STAGE_BUDGET = 8 * 1024;  // bytes of strip data per stage (all planes)
 
-// Words per lane of the TMA step kernel for a rule of NB planes.
-template <int NB>
+// Words per lane of the TMA step kernel for a rule of NB planes in a layout:
+// 4 for one-plane rules, 2 for two or three planes, else 1; and 1 in the
+// 8-row tiled layout, whose eight rows per word already give each lane enough
+// independent work (two words there cost registers and occupancy: on B200,
+// WireWorld 0.50 against 0.55 and Greenberg-Hastings 0.50 against 0.65 of
+// the HBM peak at 16384^2).
+template <int NB, int LAYOUT>
 constexpr int tma_default_v() {
-    return NB == 1 ? 4 : (NB <= 3 ? 2 : 1);
+    return LAYOUT == LAYOUT_TILED8 ? 1 : (NB == 1 ? 4 : (NB <= 3 ? 2 : 1));
 }
 
 // Geometry and shared-memory layout of the kernel for (NB, LAYOUT, V).
