@@ -68,24 +68,29 @@ CPU_SAMPLE_SIZE = 2048
 # sources it was captured from (kernel_source_hash); an entry whose hash no
 # longer matches the sources is reported as stale and not used.
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 8, 16384): (84.97e6, "profiles/temporal_kernel_wire_tiled64_16384_k8.md", None),
-    ("wire", "temporal", 16, 16384): (82.89e6, "profiles/temporal_kernel_wire_tiled64_16384_k16.md", None),
-    ("excitable", "temporal", 16, 16384): (151.17e6, "profiles/temporal_kernel_excitable_tiled64_16384_k16.md", None),
-    ("cyclic", "temporal", 16, 32768): (1295.33e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md", None),
-    ("fluid", "temporal", 16, 32768): (1028.18e6, "profiles/dram_temporal_kernel_cyclic_fluid_linear_32768_k16.md", None),
+    ("wire", "temporal", 12, 16384): (87.36e6, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
+    ("wire", "temporal", 16, 16384): (87.10e6, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
+    ("excitable", "temporal", 16, 16384): (152.54e6, "profiles/temporal_kernel_dram_alu_captures.md", "2239110cdd4f5090"),
+    ("cyclic", "temporal", 8, 32768): (1293.32e6, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
+    ("cyclic", "temporal", 16, 32768): (1293.15e6, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
+    ("fluid", "temporal", 16, 32768): (1025.06e6, "profiles/temporal_kernel_dram_alu_captures.md", "4a24be5afc467c9f"),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
 # temporal kernel configuration, from one ncu capture of that configuration
 # (summary in profiles/); keyed by (rule, layout, word size, k, tile_rows, row
-# loop, words per lane, size), tile_rows 0 being the library's default height.  Each
-# configuration is timed live and set against the ALU pipe's measured rate
+# loop, words per lane, size), tile_rows 0 being the library's default height.
+# Each configuration is timed live and set against the ALU pipe's measured rate
 # (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 64, 16, 0, 2, 1, 16384): (129431808, "profiles/alu_pipe_temporal_kernels.md", None),
-    ("excitable", 1, 64, 16, 0, 2, 1, 16384): (70207344, "profiles/alu_pipe_temporal_kernels.md", None),
-    ("cyclic", 0, 64, 16, 0, 2, 1, 32768): (1664571440, "profiles/alu_pipe_temporal_kernels.md", None),
-    ("fluid", 0, 64, 16, 0, 2, 1, 32768): (312104380, "profiles/alu_pipe_temporal_kernels.md", None),
+    ("wire", 1, 32, 12, 0, 2, 1, 16384): (97716096, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
+    ("wire", 1, 32, 16, 0, 2, 1, 16384): (130637808, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
+    ("wire", 1, 64, 16, 0, 2, 1, 16384): (129431808, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
+    ("excitable", 1, 32, 16, 0, 2, 1, 16384): (71831952, "profiles/temporal_kernel_dram_alu_captures.md", "2239110cdd4f5090"),
+    ("excitable", 1, 64, 16, 0, 2, 1, 16384): (70207344, "profiles/temporal_kernel_dram_alu_captures.md", "2239110cdd4f5090"),
+    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
+    ("cyclic", 0, 64, 16, 0, 2, 1, 32768): (1664571440, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
+    ("fluid", 0, 64, 16, 0, 2, 1, 32768): (312104380, "profiles/temporal_kernel_dram_alu_captures.md", "4a24be5afc467c9f"),
 }
 
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
