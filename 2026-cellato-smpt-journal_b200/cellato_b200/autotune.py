@@ -34,7 +34,8 @@ import threading
 from . import lib
 
 # (mode, k[, tile_rows[, row loop[, words per lane]]]); tile_rows 0 = the
-# library's default height for k; row loop as cellato_tune.row_loop and words
+# library's default height for k; row loop as cellato_tune.row_loop (1 row by
+# row, 2 hoisted, 3 two steps per sweep) and words
 # per lane as cellato_tune.words_per_lane (0 = default; two words per lane exist
 # only for rules of up to three planes, and are skipped for the others).
 # Single-step candidates: the single-step kernels and the temporal kernel at
@@ -42,9 +43,9 @@ from . import lib
 # many planes or long networks reaches more of the HBM roofline.
 SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1), ("simple_tma", 1)) + tuple(
     ("temporal", 1, th, loop, width) for th in (0, 96, 128, 192) for loop in (1, 2) for width in (1, 2))
-DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2),) + tuple(
+DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2), ("temporal", 2, 0, 3)) + tuple(
     ("temporal", k, th, loop, width) for k in (4, 6, 8, 12, 16, 24) for th in (0, 96, 128, 160, 192, 256, 320)
-    for loop in (1, 2) for width in (1, 2))
+    for loop in (1, 2, 3) for width in (1, 2))
 _VARIANT = {"simple": 0, "simple_register": 1, "simple_stream": 2, "simple_tma": 3}
 
 TIE_BAND = 0.02   # candidates within 2% of the fastest are ties

@@ -77,7 +77,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("waiting", ctypes.c_longlong), ("running", ctypes.c_longlong), ("active", ctypes.c_longlong),
                 ("completed_unpolled", ctypes.c_longlong), ("resident_bytes", ctypes.c_ulonglong),
                 ("hbm_cap_bytes", ctypes.c_ulonglong), ("iterations", ctypes.c_longlong),
-                ("kernel_launches", ctypes.c_longlong), ("cell_steps", ctypes.c_double)]
+                ("kernel_launches", ctypes.c_longlong), ("cell_steps", ctypes.c_double),
+                ("pool_trims", ctypes.c_longlong)]
 
 
 _lib = None

@@ -251,7 +251,7 @@ static int check_tune(const cellato_tune* t) {
     if (!t) return CELLATO_OK;
     if (t->simple_kernel < 0 || t->simple_kernel > 3)
         return fail(CELLATO_EINVAL, "tune.simple_kernel must be 0, 1, 2 or 3 (got %d)", t->simple_kernel);
-    if (t->row_loop < 0 || t->row_loop > 2) return fail(CELLATO_EINVAL, "tune.row_loop must be 0, 1 or 2 (got %d)", t->row_loop);
+    if (t->row_loop < 0 || t->row_loop > 3) return fail(CELLATO_EINVAL, "tune.row_loop must be 0 to 3 (got %d)", t->row_loop);
     if (t->words_per_lane < 0 || t->words_per_lane > 2)
         return fail(CELLATO_EINVAL, "tune.words_per_lane must be 0, 1 or 2 (got %d)", t->words_per_lane);
     if (t->tile_rows < 0) return fail(CELLATO_EINVAL, "tune.tile_rows must be >= 0 (got %d)", t->tile_rows);

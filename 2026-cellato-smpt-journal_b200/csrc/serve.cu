@@ -88,7 +88,7 @@ struct cellato_server_st {
     std::deque<inflight_rec> inflight;
     std::unordered_map<long long, req_rec> recs;
     std::deque<cellato_server_result> completed;
-    long long iterations = 0, launches = 0, last_active = 0;
+    long long iterations = 0, launches = 0, last_active = 0, pool_trims = 0;
     double cell_steps = 0;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     bool broken = false;
@@ -172,6 +172,22 @@ int drain(cellato_server_st* s) {
     return CELLATO_OK;
 }
 
+// A block of the server's pool, stream-ordered on the main stream.  The pool
+// keeps freed blocks for later admissions; over a long stream of mixed sizes
+// they fragment, and the pool can run out of device memory while the resident
+// total is within the cap.  Then the frees already issued are completed, the
+// pool's unused blocks are returned to the device, and the allocation is tried
+// once more.
+cudaError_t pool_alloc(cellato_server_st* s, void** p, size_t bytes) {
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, s->pool, s->main_stream);
+    if (e != cudaErrorMemoryAllocation) return e;
+    (void)cudaGetLastError();
+    if ((e = cudaStreamSynchronize(s->main_stream)) != cudaSuccess) return e;
+    if ((e = cudaMemPoolTrimTo(s->pool, 0)) != cudaSuccess) return e;
+    ++s->pool_trims;
+    return cudaMallocFromPoolAsync(p, bytes, s->pool, s->main_stream);
+}
+
 int ensure_slot(cellato_server_st* s, slot& sl, size_t bytes) {
     if (sl.host_cap < bytes) {
         if (sl.host) cudaFreeHost(sl.host);
@@ -187,8 +203,7 @@ int ensure_slot(cellato_server_st* s, slot& sl, size_t bytes) {
         sl.dev = nullptr;
         sl.dev_cap = 0;
         const size_t cap = round_up(bytes + bytes / 2, 1 << 16);
-        const cudaError_t e =
-            cudaMallocFromPoolAsync(reinterpret_cast<void**>(&sl.dev), cap, s->pool, s->main_stream);
+        const cudaError_t e = pool_alloc(s, reinterpret_cast<void**>(&sl.dev), cap);
         if (e != cudaSuccess) return server_cuda_fail(s, e, "cudaMallocFromPoolAsync (server work list)");
         sl.dev_cap = cap;
     }
@@ -199,7 +214,7 @@ int ensure_slot(cellato_server_st* s, slot& sl, size_t bytes) {
 int materialise(cellato_server_st* s, long long id) {
     req_rec& r = s->recs[id];
     const size_t bytes = 2 * (size_t)r.nb * r.stride;
-    cudaError_t e = cudaMallocFromPoolAsync(&r.base, bytes, s->pool, s->main_stream);
+    cudaError_t e = pool_alloc(s, &r.base, bytes);
     if (e != cudaSuccess) return server_cuda_fail(s, e, "cudaMallocFromPoolAsync (request planes)");
     auto* b = static_cast<unsigned char*>(r.base);
     for (int p = 0; p < r.nb; ++p) {
@@ -595,6 +610,7 @@ int cellato_server_stats_get(cellato_server_t s, cellato_server_stats* st) {
     st->iterations = s->iterations;
     st->kernel_launches = s->launches;
     st->cell_steps = s->cell_steps;
+    st->pool_trims = s->pool_trims;
     return CELLATO_OK;
 }
 

@@ -636,7 +636,8 @@ __global__ void __launch_bounds__(WARPS * 32) stream_step_kernel(plane_set in, p
 // depends on the rule's register use and the occupancy (the autotuner picks).
 // LOAD: how the tile is read from global memory (LOAD_NC, or LOAD_CG when the
 // input may have been written earlier in the same launch).
-template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST = true, int LOAD = LOAD_NC>
+// PAIR: two steps per sweep (see pair_step); an odd last step runs alone.
+template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST = true, int LOAD = LOAD_NC, bool PAIR = false>
 __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                                               int TH, int HY, int bx, int by) {
     constexpr int R = band_rows<LAYOUT>();
@@ -830,7 +831,142 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
         __syncthreads();
     };
 
-    for (int t = 1; t <= k; ++t) {
+    // Two steps per sweep: steps t and t+1 of a warp's band in one top-down
+    // pass.  The band is cut from the rows step t+1 computes (t+1 .. TH-2-t);
+    // step t's values of the band's rows and of the row on either side of it
+    // are computed in registers from the old rows, two on either side of the
+    // band read before the first barrier, and only step t+1's rows are written
+    // back.  Per two steps a row is read from and written to shared memory
+    // once instead of twice; the two step-t rows at each band edge are
+    // computed by both neighbouring warps.  Rows t and TH-1-t keep their older
+    // values, which no later step reads.  The values are the ones two single
+    // steps give, halo words included.
+    auto eval_words = [&](auto tp_tag, const feat (&fu)[V], const feat (&fm)[V], const feat (&fd)[V], int gy,
+                          word (&o)[NB][V]) {
+        constexpr int TP = decltype(tp_tag)::value;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            word ov[NB];
+            Net::template eval<TP>(fu[v], fm[v], fd[v], gy & 1, ov);
+#pragma unroll
+            for (int p = 0; p < NB; ++p) o[p][v] = ov[p];
+        }
+    };
+    auto pair_step = [&](int t, auto tp_tag) {
+        constexpr int TP = decltype(tp_tag)::value;
+        const std::integral_constant<int, TP ^ 1> tp2{};
+        const int total = TH - 2 * (t + 1);
+        const int base = total / WARPS, extra = total % WARPS;
+        const int lo = t + 1 + warp * base + min(warp, extra);
+        const int hi = lo + base + (warp < extra ? 1 : 0);
+        word A0[NB][V], A1[NB][V], B0[NB][V], B1[NB][V];  // old rows lo-2, lo-1, hi, hi+1
+        if (lo < hi) {
+            read_row(lo - 2, A0);
+            read_row(lo - 1, A1);
+            read_row(hi, B0);
+            read_row(hi + 1, B1);
+        }
+        __syncthreads();
+        if (lo < hi) {
+            // E*: features of old rows; H*: features of step-t rows
+            feat E0[V], E1[V], E2[V], H0[V], H1[V], H2[V];
+            int gy = (y0 - HY + lo) % Y;  // global row of tile row r
+            if (gy < 0) gy += Y;
+            auto next_gy = [&](int g) { return g + 1 == Y ? 0 : g + 1; };
+            const int gy_up = gy == 0 ? Y - 1 : gy - 1;
+            {
+                word o[NB][V];
+                feats(A0, E0);
+                feats(A1, E1);
+                read_row(lo, o);
+                feats(o, E2);
+                eval_words(tp_tag, E0, E1, E2, gy_up, o);  // step t, row lo-1
+                feats(o, H0);
+                if (lo + 1 < hi) {
+                    read_row(lo + 1, o);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < NB; ++p)
+#pragma unroll
+                        for (int v = 0; v < V; ++v) o[p][v] = B0[p][v];
+                }
+                feats(o, E0);
+                eval_words(tp_tag, E1, E2, E0, gy, o);  // step t, row lo
+                feats(o, H1);
+            }
+            // Output row r: old rows r, r+1 in Ea, Eb and r+2 in C; step-t
+            // rows r-1, r in Ha, Hb.  Computes step t of row r+1 into Hc and
+            // step t+1 of row r, written in place (old row r is no longer read).
+            auto body = [&](int r, int g, const word (&C)[NB][V], const feat (&Ea)[V], const feat (&Eb)[V],
+                            feat (&Ec)[V], const feat (&Ha)[V], const feat (&Hb)[V], feat (&Hc)[V]) {
+                word o[NB][V];
+                feats(C, Ec);
+                eval_words(tp_tag, Ea, Eb, Ec, next_gy(g), o);
+                feats(o, Hc);
+                eval_words(tp2, Ha, Hb, Hc, g, o);
+                write_row(r, o);
+            };
+            // old row x (lo <= x <= hi + 1): the band's own rows from shared
+            // memory, the two below it from the rows saved before the barrier
+            auto old_row = [&](int x, word (&C)[NB][V]) {
+                if (x < hi) {
+                    read_row(x, C);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < NB; ++p)
+#pragma unroll
+                        for (int v = 0; v < V; ++v) C[p][v] = x == hi ? B0[p][v] : B1[p][v];
+                }
+            };
+            int r = lo;
+            // feature sets rotate by name over a trip of three rows; the
+            // trip's three old rows are read before any of its writes
+            for (; r + 4 < hi; r += 3) {
+                word C1[NB][V], C2[NB][V], C3[NB][V];
+                read_row(r + 2, C1);
+                read_row(r + 3, C2);
+                read_row(r + 4, C3);
+                body(r, gy, C1, E2, E0, E1, H0, H1, H2);
+                gy = next_gy(gy);
+                body(r + 1, gy, C2, E0, E1, E2, H1, H2, H0);
+                gy = next_gy(gy);
+                body(r + 2, gy, C3, E1, E2, E0, H2, H0, H1);
+                gy = next_gy(gy);
+            }
+            // the band's last one to four rows
+            auto tail = [&](int rr, int g, const feat (&Ea)[V], const feat (&Eb)[V], feat (&Ec)[V],
+                            const feat (&Ha)[V], const feat (&Hb)[V], feat (&Hc)[V]) {
+                word C[NB][V];
+                old_row(rr + 2, C);
+                body(rr, g, C, Ea, Eb, Ec, Ha, Hb, Hc);
+            };
+            if (r < hi) {
+                tail(r, gy, E2, E0, E1, H0, H1, H2);
+                gy = next_gy(gy);
+                if (r + 1 < hi) {
+                    tail(r + 1, gy, E0, E1, E2, H1, H2, H0);
+                    gy = next_gy(gy);
+                    if (r + 2 < hi) {
+                        tail(r + 2, gy, E1, E2, E0, H2, H0, H1);
+                        gy = next_gy(gy);
+                        if (r + 3 < hi) tail(r + 3, gy, E2, E0, E1, H0, H1, H2);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    };
+
+    int t = 1;
+    if constexpr (PAIR) {
+        for (; t + 1 <= k; t += 2) {
+            if (((t0 + t - 1) & 1) == 0)
+                pair_step(t, std::integral_constant<int, 0>{});
+            else
+                pair_step(t, std::integral_constant<int, 1>{});
+        }
+    }
+    for (; t <= k; ++t) {
         if (((t0 + t - 1) & 1) == 0)
             step(t, std::integral_constant<int, 0>{});
         else
@@ -857,10 +993,11 @@ __device__ __forceinline__ void temporal_tile(const plane_set& in, const plane_s
     }
 }
 
-template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST>
+template <class Net, int NB, int LAYOUT, int V, int WARPS, bool HOIST, bool PAIR = false>
 __global__ void __launch_bounds__(WARPS * 32) temporal_kernel(plane_set in, plane_set out, int Xw, int Y, int t0,
                                                               int k, int TH, int HY) {
-    temporal_tile<Net, NB, LAYOUT, V, WARPS, HOIST>(in, out, Xw, Y, t0, k, TH, HY, blockIdx.x, blockIdx.y);
+    temporal_tile<Net, NB, LAYOUT, V, WARPS, HOIST, LOAD_NC, PAIR>(in, out, Xw, Y, t0, k, TH, HY, blockIdx.x,
+                                                                    blockIdx.y);
 }
 
 // ======================================================= batched temporal kernel

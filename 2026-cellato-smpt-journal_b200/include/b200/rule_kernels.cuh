@@ -31,7 +31,7 @@ namespace cellato::b200 {
 // Single-step kernel choices (cellato_tune::simple_kernel).
 enum : int { SIMPLE_AUTO = 0, SIMPLE_REGISTER = 1, SIMPLE_STREAM = 2, SIMPLE_TMA = 3 };
 // Temporal row loops (cellato_tune::row_loop).
-enum : int { LOOP_AUTO = 0, LOOP_ROW_BY_ROW = 1, LOOP_HOISTED = 2 };
+enum : int { LOOP_AUTO = 0, LOOP_ROW_BY_ROW = 1, LOOP_HOISTED = 2, LOOP_PAIRED = 3 };
 }  // namespace cellato::b200
 
 // The kernels of one rule, as function pointers into the translation unit that
@@ -227,6 +227,7 @@ struct rule_kernels {
     static cudaError_t temporal_launch(const plane_set& in, const plane_set& out, int Xw, int Y, int t0, int k,
                                        int TH, int HY, int loop, cudaStream_t s) {
         auto kern = loop == LOOP_ROW_BY_ROW ? temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, false>
+                    : loop == LOOP_PAIRED   ? temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, true, true>
                                             : temporal_kernel<net, NB, LAYOUT, V, TEMPORAL_WARPS, true>;
         const size_t smem = (size_t)NB * TH * 32 * V * sizeof(word);
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -347,7 +347,7 @@ def describe_choice(c: dict) -> str:
     w = f" W{c['word_bits']}" if "word_bits" in c else ""
     if c["mode"] != "temporal":
         return c["mode"] + w
-    loop = {0: "default", 1: "row-by-row", 2: "hoisted"}[c.get("loop", 0)]
+    loop = {0: "default", 1: "row-by-row", 2: "hoisted", 3: "paired"}[c.get("loop", 0)]
     width = {0: "default", 1: "1", 2: "2"}[c.get("width", 0)]
     return f"temporal k={c['k']} tile_rows={c.get('tile_rows', 0)} loop={loop} words_per_lane={width}{w}"
 
@@ -954,7 +954,8 @@ def served_arm(args, rank: int, world: int):
         "per_grid": base,
         "served_over_per_grid": round(value / world / base["gcups"], 2) if base else None,
         "sample_bit_exact": f"{sample_ok}/{len(sample)}",
-        "server": {"iterations": stats["iterations"], "kernel_launches": stats["kernel_launches"]},
+        "server": {"iterations": stats["iterations"], "kernel_launches": stats["kernel_launches"],
+                   "pool_trims": stats["pool_trims"]},
         "e2e": {"value": round(value, 1), "unit": "GCUPS", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": 128 * n,
                 "note": "requests enter through the server's C ABI as seeds; results leave as 16 tile sums each"},

@@ -93,7 +93,8 @@ typedef struct {
                             layout, rows of 16-byte multiples; others use 1), 3 TMA-fed shared-memory tiles
                             (rows of a multiple of 4096 cells; others use 1) */
     int row_loop;        /* temporal row loop: 0 automatic, 1 row by row, 2 the input rows of each three-row
-                            trip read before its in-place writes */
+                            trip read before its in-place writes, 3 as 2 with two steps per sweep of the
+                            tile (an odd last step runs alone) */
     int words_per_lane;  /* temporal tile width: 0 the rule's default (2 for one-plane rules, else 1), 1, or 2
                             (rules of up to three planes; others use 1); the tile is 32 x this many words */
     int tile_rows;       /* temporal tile rows including both k-row halos; 0 the library's default */
@@ -379,6 +380,8 @@ typedef struct {
     unsigned long long resident_bytes, hbm_cap_bytes;
     long long iterations, kernel_launches;
     double cell_steps;                /* cell updates enqueued since creation */
+    long long pool_trims;             /* times a plane allocation found the pool fragmented: issued frees
+                                         were completed, unused blocks returned, the allocation retried */
 } cellato_server_stats;
 
 int cellato_server_create(const cellato_server_config* config, cellato_server_t* out);

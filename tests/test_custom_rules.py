@@ -133,10 +133,12 @@ def _run(rule, layout, W, cells, steps, mode, k=1, t0=0, **tune):
 @pytest.mark.gpu
 @pytest.mark.parametrize("layout,W", LAYOUTS)
 def test_custom_rules_on_gpu_match_reference(cuda, custom_ids, custom_cases, layout, W):
-    """Single-step kernels (both) and the temporal kernel (k = 1, 3, 8, 16,
-    both row loops and widths) on the custom rules against the reference."""
+    """Single-step kernels (both) and the temporal kernel (k = 1, 3, 5, 8, 16,
+    the three row loops and both widths) on the custom rules against the
+    reference."""
     runs = [("simple", 1, {}), ("simple", 1, {"simple_kernel": 2}), ("temporal", 1, {}), ("temporal", 3, {}),
-            ("temporal", 8, {"row_loop": 1, "words_per_lane": 2}), ("temporal", 16, {"row_loop": 2})]
+            ("temporal", 8, {"row_loop": 1, "words_per_lane": 2}), ("temporal", 16, {"row_loop": 2}),
+            ("temporal", 5, {"row_loop": 3}), ("temporal", 8, {"row_loop": 3, "words_per_lane": 2})]
     for case, cin, cout in custom_cases:
         rid = custom_ids[case["rule"]]
         for mode, k, tune in runs:

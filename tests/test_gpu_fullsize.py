@@ -60,7 +60,9 @@ def checksum(rule, layout, p, X, Y):
 
 @pytest.mark.parametrize("rule,k,th,loop,width", [("wire", 8, 128, 1, 0), ("wire", 16, 0, 2, 0),
                                                   ("excitable", 16, 0, 2, 0), ("excitable", 8, 128, 1, 0),
-                                                  ("excitable", 16, 192, 2, 2), ("wire", 16, 192, 1, 1)])
+                                                  ("excitable", 16, 192, 2, 2), ("wire", 16, 192, 1, 1),
+                                                  ("wire", 12, 0, 3, 0), ("excitable", 16, 0, 3, 0),
+                                                  ("excitable", 24, 256, 3, 2)])
 def test_config2_size_temporal_equals_single_step(cuda, rule, k, th, loop, width):
     import torch
     r = lib.rule_id(rule)
@@ -90,13 +92,14 @@ def test_config2_size_layouts_agree_on_checksums(cuda):
 @pytest.mark.parametrize("rule", ["cyclic", "fluid"])
 def test_config3_size_temporal_equals_single_step(cuda, rule):
     """Every depth the config-3 workload lets the autotuner choose (k <= 32) at
-    the library's default tile height and both row loops, plus the k = 1
+    the library's default tile height and the three row loops, plus the k = 1
     single-step candidate, against the single-step kernel on 32768^2."""
     import torch
     r = lib.rule_id(rule)
     S, steps = 32768, 64
     ref = run(r, 0, S, S, steps, 42, "simple")
-    for k, th, loop in ((16, 0, 2), (16, 0, 1), (24, 0, 2), (32, 0, 2), (12, 0, 2), (8, 0, 2), (1, 128, 1)):
+    for k, th, loop in ((16, 0, 2), (16, 0, 1), (24, 0, 2), (32, 0, 2), (12, 0, 2), (8, 0, 2), (1, 128, 1),
+                        (16, 0, 3), (24, 0, 3), (8, 160, 3)):
         got = run(r, 0, S, S, steps, 42, "temporal", k, th, loop)
         assert diff(inputs.PLANES[r], ref, got) == 0, (rule, k, th, loop)
         del got

@@ -52,12 +52,14 @@ def test_temporal_small_golden(cuda, oracle, golden_small, layout, W, k):
 
 
 @pytest.mark.parametrize("width", [1, 2])
-@pytest.mark.parametrize("loop", [1, 2])
-@pytest.mark.parametrize("k", [3, 8, 24, 32])
+@pytest.mark.parametrize("loop", [1, 2, 3])
+@pytest.mark.parametrize("k", [2, 3, 8, 24, 32])
 @pytest.mark.parametrize("layout,W", LAYOUTS)
 def test_temporal_row_loops(cuda, oracle, golden_small, layout, W, k, loop, width):
-    """Both row loops (cellato_tune.row_loop) and both tile widths
-    (cellato_tune.words_per_lane) of the temporal kernel."""
+    """The three row loops (cellato_tune.row_loop: row by row, hoisted, two
+    steps per sweep -- odd k ends with a single step) and both tile widths
+    (cellato_tune.words_per_lane) of the temporal kernel.  The tiles are the
+    shortest allowed, so late steps leave warps bands of zero to four rows."""
     # the shortest tile that leaves 16 interior rows below the two k-row halos
     th = max(48, 2 * ((k + 7) // 8 * 8) + 16)
     for case, cin, cout in golden_small:
@@ -67,10 +69,12 @@ def test_temporal_row_loops(cuda, oracle, golden_small, layout, W, k, loop, widt
         assert np.array_equal(out, cout), (case["key"], case["rule"], k, loop, width)
 
 
-@pytest.mark.parametrize("mode,k", [("simple", 1), ("temporal", 3), ("temporal", 8)])
+@pytest.mark.parametrize("mode,k,loop", [("simple", 1, 0), ("temporal", 3, 0), ("temporal", 8, 0), ("temporal", 3, 3),
+                                         ("temporal", 8, 3)])
 @pytest.mark.parametrize("t0", [1, 2, 7])
-def test_step_parity_offsets(cuda, oracle, mode, k, t0):
-    """alternate_algorithms and Margolus phase follow the global step number."""
+def test_step_parity_offsets(cuda, oracle, mode, k, loop, t0):
+    """alternate_algorithms and Margolus phase follow the global step number
+    (also when two steps share a sweep, loop 3)."""
     rng = np.random.default_rng(t0)
     for r in range(10):
         cells = rng.integers(0, inputs.STATES[r], size=(40, 128), dtype=np.uint8)
@@ -78,8 +82,8 @@ def test_step_parity_offsets(cuda, oracle, mode, k, t0):
         for layout, W in [(0, 32), (1, 64)]:
             if layout == 1 and 40 % (W // 8):
                 continue
-            got = run_gpu(oracle, r, layout, W, cells, 11, mode=mode, k=k, t0=t0)
-            assert np.array_equal(got, want), (RULES[r], layout, W, t0)
+            got = run_gpu(oracle, r, layout, W, cells, 11, mode=mode, k=k, t0=t0, row_loop=loop)
+            assert np.array_equal(got, want), (RULES[r], layout, W, t0, loop)
 
 
 def test_odd_heights_and_narrow_rows(cuda, oracle):
