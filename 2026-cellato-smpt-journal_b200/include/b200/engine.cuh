@@ -1034,7 +1034,7 @@ constexpr int BATCH_STEPS_MASK = 0xff;
 constexpr int BATCH_FLIP_BUFFER = 1 << 8;
 constexpr int BATCH_FLIP_TIME = 1 << 9;
 constexpr int BATCH_ROUND_SHIFT = 10;
-constexpr unsigned BATCH_WAIT_LIMIT = 1u << 24;  // polls of 64 ns sleeps: about a second
+constexpr unsigned BATCH_WAIT_LIMIT = 1u << 24;  // polls with 64 ns sleeps: seconds, far above any round's time
 
 __device__ __forceinline__ unsigned load_acquire_gpu(const unsigned* p) {
     unsigned v;
@@ -1043,12 +1043,15 @@ __device__ __forceinline__ unsigned load_acquire_gpu(const unsigned* p) {
 }
 
 // head: the launch's queue head; done[g]: finished tiles of grid g.  Both start
-// at zero (the host clears them before the launch).
-template <class Net, int NB, int LAYOUT, int V, int WARPS>
+// at zero (the host clears them before the launch).  wait_limit: polls before
+// a wait gives up (BATCH_WAIT_LIMIT in the library).  PAIR: tiles run two
+// steps per sweep.
+template <class Net, int NB, int LAYOUT, int V, int WARPS, bool PAIR>
 __global__ void __launch_bounds__(WARPS * 32) temporal_batch_kernel(const batch_grid_desc* __restrict__ grids,
                                                                     const batch_item* __restrict__ items, int n_items,
                                                                     int parity, int t0, int TH, int HY,
-                                                                    unsigned* head, unsigned* done) {
+                                                                    unsigned* head, unsigned* done,
+                                                                    unsigned wait_limit) {
     __shared__ int s_item;
     for (;;) {
         if (threadIdx.x == 0) s_item = (int)atomicAdd(head, 1u);
@@ -1062,7 +1065,7 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_batch_kernel(const batch_
             const unsigned need = round * (unsigned)g.tiles;
             unsigned polls = 0;
             while (load_acquire_gpu(done + it.grid) < need) {
-                if (++polls == BATCH_WAIT_LIMIT) {
+                if (++polls >= wait_limit) {
                     atomicAdd(&g_wait_timeouts, 1u);
                     break;
                 }
@@ -1072,8 +1075,9 @@ __global__ void __launch_bounds__(WARPS * 32) temporal_batch_kernel(const batch_
         __syncthreads();
         const int src = parity ^ ((it.steps & BATCH_FLIP_BUFFER) ? 1 : 0);
         const int start = t0 + ((it.steps & BATCH_FLIP_TIME) ? 1 : 0);
-        temporal_tile<Net, NB, LAYOUT, V, WARPS, true, LOAD_CG>(g.p[src], g.p[src ^ 1], g.Xw, g.Y, start,
-                                                               it.steps & BATCH_STEPS_MASK, TH, HY, it.tx, it.ty);
+        temporal_tile<Net, NB, LAYOUT, V, WARPS, true, LOAD_CG, PAIR>(g.p[src], g.p[src ^ 1], g.Xw, g.Y, start,
+                                                                     it.steps & BATCH_STEPS_MASK, TH, HY, it.tx,
+                                                                     it.ty);
         // publish the tile: every thread's stores are visible device-wide
         // before the count that releases the next round
         __threadfence();

@@ -951,8 +951,7 @@ struct signal_layout<Dict, tlist<Ss...>> {
     template <class S>
     static constexpr int offset() {
         int off = 0, found = -1;
-        ((std::is_same_v<S, Ss> ? (found = found < 0 ? off : found, 0) : 0, off += signal_width<Dict, Ss>::value),
-         ...);
+        ((found = (std::is_same_v<S, Ss> && found < 0) ? off : found, off += signal_width<Dict, Ss>::value), ...);
         return found;
     }
 };

@@ -96,6 +96,8 @@ struct rule_kernels {
     // which wastes less on the narrow grids of a batch, and its register use
     // leaves room for three CTAs per SM.
     static constexpr int BATCH_V = 1;
+    // ... and two steps per sweep of a tile (row loop 3)
+    static constexpr bool BATCH_PAIR = true;
     static constexpr int TEMPORAL_WARPS = 8;
 
     template <int LAYOUT, int V>
@@ -259,7 +261,7 @@ struct rule_kernels {
 
     template <int LAYOUT>
     static auto batch_kernel() {
-        return temporal_batch_kernel<net, NB, LAYOUT, BATCH_V, TEMPORAL_WARPS>;
+        return temporal_batch_kernel<net, NB, LAYOUT, BATCH_V, TEMPORAL_WARPS, BATCH_PAIR>;
     }
     static size_t tile_smem(int TH) { return (size_t)NB * TH * 32 * BATCH_V * sizeof(word); }
 
@@ -303,15 +305,15 @@ struct rule_kernels {
         switch (layout) {
             case LAYOUT_LINEAR:
                 batch_kernel<LAYOUT_LINEAR>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY,
-                                                                        head, done);
+                                                                        head, done, BATCH_WAIT_LIMIT);
                 break;
             case LAYOUT_TILED4:
                 batch_kernel<LAYOUT_TILED4>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY,
-                                                                        head, done);
+                                                                        head, done, BATCH_WAIT_LIMIT);
                 break;
             case LAYOUT_TILED8:
                 batch_kernel<LAYOUT_TILED8>()<<<grid, block, smem, s>>>(grids, items, n_items, parity, t0, TH, HY,
-                                                                        head, done);
+                                                                        head, done, BATCH_WAIT_LIMIT);
                 break;
             default:
                 return cudaErrorInvalidValue;

@@ -68,12 +68,10 @@ CPU_SAMPLE_SIZE = 2048
 # sources it was captured from (kernel_source_hash); an entry whose hash no
 # longer matches the sources is reported as stale and not used.
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 12, 16384): (87.36e6, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
-    ("wire", "temporal", 16, 16384): (87.10e6, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
-    ("excitable", "temporal", 16, 16384): (152.54e6, "profiles/temporal_kernel_dram_alu_captures.md", "2239110cdd4f5090"),
-    ("cyclic", "temporal", 8, 32768): (1293.32e6, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
-    ("cyclic", "temporal", 16, 32768): (1293.15e6, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
-    ("fluid", "temporal", 16, 32768): (1025.06e6, "profiles/temporal_kernel_dram_alu_captures.md", "4a24be5afc467c9f"),
+    ("wire", "temporal", 12, 16384): (87.34e6, "profiles/temporal_kernel_dram_alu_captures.md", "6e7165e6054cc5cd"),
+    ("excitable", "temporal", 16, 16384): (152.93e6, "profiles/temporal_kernel_dram_alu_captures.md", "4bd271d08768106a"),
+    ("cyclic", "temporal", 8, 32768): (1293.69e6, "profiles/temporal_kernel_dram_alu_captures.md", "4d616ed2498b26a1"),
+    ("fluid", "temporal", 16, 32768): (1025.51e6, "profiles/temporal_kernel_dram_alu_captures.md", "501b6d5b0c8e008b"),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
@@ -83,14 +81,10 @@ MEASURED_TRAFFIC = {
 # Each configuration is timed live and set against the ALU pipe's measured rate
 # (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 32, 12, 0, 2, 1, 16384): (97716096, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
-    ("wire", 1, 32, 16, 0, 2, 1, 16384): (130637808, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
-    ("wire", 1, 64, 16, 0, 2, 1, 16384): (129431808, "profiles/temporal_kernel_dram_alu_captures.md", "b6d919a7a096c3a8"),
-    ("excitable", 1, 32, 16, 0, 2, 1, 16384): (71831952, "profiles/temporal_kernel_dram_alu_captures.md", "2239110cdd4f5090"),
-    ("excitable", 1, 64, 16, 0, 2, 1, 16384): (70207344, "profiles/temporal_kernel_dram_alu_captures.md", "2239110cdd4f5090"),
-    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
-    ("cyclic", 0, 64, 16, 0, 2, 1, 32768): (1664571440, "profiles/temporal_kernel_dram_alu_captures.md", "18d6d1048978d604"),
-    ("fluid", 0, 64, 16, 0, 2, 1, 32768): (312104380, "profiles/temporal_kernel_dram_alu_captures.md", "4a24be5afc467c9f"),
+    ("wire", 1, 32, 12, 0, 3, 1, 16384): (98888256, "profiles/temporal_kernel_dram_alu_captures.md", "6e7165e6054cc5cd"),
+    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (72008352, "profiles/temporal_kernel_dram_alu_captures.md", "4bd271d08768106a"),
+    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "4d616ed2498b26a1"),
+    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "501b6d5b0c8e008b"),
 }
 
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",

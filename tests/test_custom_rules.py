@@ -13,6 +13,7 @@ import ctypes
 import json
 import os
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -232,3 +233,21 @@ def test_two_threads_two_streams_different_tunings(cuda):
     for t in threads:
         t.join()
     assert not errors, errors
+
+
+@pytest.mark.gpu
+def test_batch_wait_that_runs_out_returns_and_counts(cuda, custom_ids):
+    """Failure handling of the persistent batch kernel's bounded waits, with
+    no device fault: an item waits for a round that is never run (a count that
+    nothing raises).  The wait gives up after its poll limit, the launch
+    returns, the timeout is counted, and the device stays usable."""
+    import torch
+    so = custom_ids["_so"]
+    so.custom_batch_wait_probe.argtypes = [ctypes.c_uint, ctypes.POINTER(ctypes.c_uint)]
+    n = ctypes.c_uint(99)
+    t = time.perf_counter()
+    assert so.custom_batch_wait_probe(4096, ctypes.byref(n)) == 0
+    assert time.perf_counter() - t < 10.0
+    assert n.value == 1
+    x = torch.arange(1024, device="cuda")
+    assert int(x.sum()) == 1024 * 1023 // 2
