@@ -37,11 +37,14 @@ from . import lib
 # library's default height for k; row loop as cellato_tune.row_loop (1 row by
 # row, 2 hoisted, 3 two steps per sweep) and words
 # per lane as cellato_tune.words_per_lane (0 = default; two words per lane exist
-# only for rules of up to three planes, and are skipped for the others).
+# only for rules of up to three planes, four only for one-plane rules, and are
+# skipped for the others; for simple_tma the width is the TMA kernel's words per
+# lane).
 # Single-step candidates: the single-step kernels and the temporal kernel at
 # k = 1 (one step per launch through a shared-memory tile), which for rules with
 # many planes or long networks reaches more of the HBM roofline.
 SINGLE_STEP_CANDIDATES = (("simple_register", 1), ("simple_stream", 1), ("simple_tma", 1)) + tuple(
+    ("simple_tma", 1, 0, 0, width) for width in (1, 2, 4)) + tuple(
     ("temporal", 1, th, loop, width) for th in (0, 96, 128, 192) for loop in (1, 2) for width in (1, 2))
 DEFAULT_CANDIDATES = SINGLE_STEP_CANDIDATES + (("temporal", 2), ("temporal", 2, 0, 3)) + tuple(
     ("temporal", k, th, loop, width) for k in (4, 6, 8, 12, 16, 24) for th in (0, 96, 128, 160, 192, 256, 320)
@@ -124,7 +127,7 @@ def legal_candidates(candidates, planes: int, max_tile_rows: dict | None = None,
         th = cand[2] if len(cand) > 2 else 0
         loop = cand[3] if len(cand) > 3 else 0
         width = cand[4] if len(cand) > 4 else 0
-        if width == 2 and planes > 3:
+        if (width == 2 and planes > 3) or (width == 4 and planes > 1):
             continue
         if th:
             halo = -(-k // band_rows) * band_rows
@@ -153,7 +156,7 @@ def run(choice: dict, rule: int, layout: int, word_bits: int, planes_a, planes_b
     """Run `steps` steps with a tuned choice; returns 1 if the result is in planes_b."""
     if choice["mode"] in _VARIANT:
         return lib.run_simple(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, stream,
-                              simple_kernel=_VARIANT[choice["mode"]])
+                              simple_kernel=_VARIANT[choice["mode"]], words_per_lane=choice.get("width", 0))
     return lib.run_temporal(rule, layout, word_bits, planes_a, planes_b, X, Y, t0, steps, choice["k"],
                             choice.get("tile_rows", 0), stream, row_loop=choice.get("loop", 0),
                             words_per_lane=choice.get("width", 0))

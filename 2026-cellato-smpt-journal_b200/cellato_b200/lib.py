@@ -78,7 +78,7 @@ class ServerStats(ctypes.Structure):
                 ("completed_unpolled", ctypes.c_longlong), ("resident_bytes", ctypes.c_ulonglong),
                 ("hbm_cap_bytes", ctypes.c_ulonglong), ("iterations", ctypes.c_longlong),
                 ("kernel_launches", ctypes.c_longlong), ("cell_steps", ctypes.c_double),
-                ("pool_trims", ctypes.c_longlong)]
+                ("pool_trims", ctypes.c_longlong), ("memory_waits", ctypes.c_longlong)]
 
 
 _lib = None
@@ -185,12 +185,13 @@ def tune(simple_kernel: int = 0, row_loop: int = 0, words_per_lane: int = 0, til
 
 
 def run_simple(rule, layout: int, word_bits: int, planes_a, planes_b, X: int, Y: int, t0: int, steps: int,
-               stream: int = 0, simple_kernel: int = 0) -> int:
+               stream: int = 0, simple_kernel: int = 0, words_per_lane: int = 0) -> int:
     """Returns 1 when the result ended in planes_b, else 0.  simple_kernel as
     cellato_tune (0 automatic, 1 register bands, 2 bulk-copy streaming, 3
-    TMA-fed shared-memory tiles)."""
+    TMA-fed shared-memory tiles); words_per_lane: the TMA kernel's (0 its
+    default)."""
     out = ctypes.c_int(0)
-    t = tune(simple_kernel=simple_kernel)
+    t = tune(simple_kernel=simple_kernel, words_per_lane=words_per_lane)
     check(load().cellato_run_simple(rule_id(rule), layout, word_bits, ptr_array(planes_a), ptr_array(planes_b),
                                     X, Y, t0, steps, ctypes.byref(t), stream, ctypes.byref(out)))
     return out.value

@@ -252,8 +252,8 @@ static int check_tune(const cellato_tune* t) {
     if (t->simple_kernel < 0 || t->simple_kernel > 3)
         return fail(CELLATO_EINVAL, "tune.simple_kernel must be 0, 1, 2 or 3 (got %d)", t->simple_kernel);
     if (t->row_loop < 0 || t->row_loop > 3) return fail(CELLATO_EINVAL, "tune.row_loop must be 0 to 3 (got %d)", t->row_loop);
-    if (t->words_per_lane < 0 || t->words_per_lane > 2)
-        return fail(CELLATO_EINVAL, "tune.words_per_lane must be 0, 1 or 2 (got %d)", t->words_per_lane);
+    if (t->words_per_lane < 0 || t->words_per_lane > 4 || t->words_per_lane == 3)
+        return fail(CELLATO_EINVAL, "tune.words_per_lane must be 0, 1, 2 or 4 (got %d)", t->words_per_lane);
     if (t->tile_rows < 0) return fail(CELLATO_EINVAL, "tune.tile_rows must be >= 0 (got %d)", t->tile_rows);
     return CELLATO_OK;
 }
@@ -271,11 +271,12 @@ int cellato_run_simple(int rule, int layout, int word_bits, void* const* planes_
     const int L = internal_layout(layout, word_bits);
     const int Xw = x_cells / 32;
     const int variant = tune ? tune->simple_kernel : SIMPLE_AUTO;
+    const int wpl = tune ? tune->words_per_lane : 0;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     for (int i = 0; i < steps; ++i) {
         const plane_set& in = (i & 1) ? b : a;
         const plane_set& out = (i & 1) ? a : b;
-        cudaError_t e = ops->simple(L, in, out, Xw, y_cells, t0 + i, variant, s);
+        cudaError_t e = ops->simple(L, in, out, Xw, y_cells, t0 + i, variant, wpl, s);
         if (e != cudaSuccess) return cuda_fail(e, "simple step launch");
     }
     if (result_in_b) *result_in_b = steps & 1;

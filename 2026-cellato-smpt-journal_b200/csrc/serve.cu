@@ -74,7 +74,8 @@ struct cellato_server_st {
     int layout = 0, word_bits = 64, internal = 0, R = 1, dev = 0, sms = 148;
     int max_inflight = 2;
     sv::scheduler sched{sv::limits{}};
-    cudaMemPool_t pool = nullptr;
+    cudaMemPool_t pool = nullptr;       // planes of requests the server drops when they finish; work lists
+    cudaMemPool_t keep_pool = nullptr;  // planes of requests kept after they finish (keep)
     cudaStream_t main_stream = nullptr;
     cudaEvent_t fork = nullptr;
     // per rule id, set up when the first request of that rule is submitted
@@ -88,7 +89,7 @@ struct cellato_server_st {
     std::deque<inflight_rec> inflight;
     std::unordered_map<long long, req_rec> recs;
     std::deque<cellato_server_result> completed;
-    long long iterations = 0, launches = 0, last_active = 0, pool_trims = 0;
+    long long iterations = 0, launches = 0, last_active = 0, pool_trims = 0, memory_waits = 0;
     double cell_steps = 0;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     bool broken = false;
@@ -122,6 +123,7 @@ void destroy_all(cellato_server_st* s) {
     if (s->fork) cudaEventDestroy(s->fork);
     if (m) cudaStreamDestroy(m);
     if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->keep_pool) cudaMemPoolDestroy(s->keep_pool);
     delete s;
 }
 
@@ -172,20 +174,23 @@ int drain(cellato_server_st* s) {
     return CELLATO_OK;
 }
 
-// A block of the server's pool, stream-ordered on the main stream.  The pool
-// keeps freed blocks for later admissions; over a long stream of mixed sizes
-// they fragment, and the pool can run out of device memory while the resident
-// total is within the cap.  Then the frees already issued are completed, the
-// pool's unused blocks are returned to the device, and the allocation is tried
-// once more.
-cudaError_t pool_alloc(cellato_server_st* s, void** p, size_t bytes) {
-    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, s->pool, s->main_stream);
+// A block of one of the server's pools, stream-ordered on the main stream.
+// The pools keep freed blocks for later admissions; over a long stream of
+// mixed sizes they fragment, and a pool can run out of device memory while the
+// resident total is within the cap.  Then the frees already issued are
+// completed, both pools' unused blocks are returned to the device, and the
+// allocation is tried once more.  Kept requests, which outlive the ones around
+// them, have a pool of their own so that they pin no blocks of the main one.
+cudaError_t pool_alloc(cellato_server_st* s, void** p, size_t bytes, bool keep = false) {
+    cudaMemPool_t pool = keep ? s->keep_pool : s->pool;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, s->main_stream);
     if (e != cudaErrorMemoryAllocation) return e;
     (void)cudaGetLastError();
     if ((e = cudaStreamSynchronize(s->main_stream)) != cudaSuccess) return e;
     if ((e = cudaMemPoolTrimTo(s->pool, 0)) != cudaSuccess) return e;
+    if ((e = cudaMemPoolTrimTo(s->keep_pool, 0)) != cudaSuccess) return e;
     ++s->pool_trims;
-    return cudaMallocFromPoolAsync(p, bytes, s->pool, s->main_stream);
+    return cudaMallocFromPoolAsync(p, bytes, pool, s->main_stream);
 }
 
 int ensure_slot(cellato_server_st* s, slot& sl, size_t bytes) {
@@ -211,10 +216,17 @@ int ensure_slot(cellato_server_st* s, slot& sl, size_t bytes) {
 }
 
 // Allocates and initialises an admitted request's planes on the main stream.
+// Returns NO_MEMORY, with nothing allocated, when the device has no room left.
+constexpr int NO_MEMORY = -1;
 int materialise(cellato_server_st* s, long long id) {
     req_rec& r = s->recs[id];
     const size_t bytes = 2 * (size_t)r.nb * r.stride;
-    cudaError_t e = pool_alloc(s, &r.base, bytes);
+    cudaError_t e = pool_alloc(s, &r.base, bytes, r.keep);
+    if (e == cudaErrorMemoryAllocation) {
+        (void)cudaGetLastError();
+        r.base = nullptr;
+        return NO_MEMORY;
+    }
     if (e != cudaSuccess) return server_cuda_fail(s, e, "cudaMallocFromPoolAsync (request planes)");
     auto* b = static_cast<unsigned char*>(r.base);
     for (int p = 0; p < r.nb; ++p) {
@@ -329,10 +341,10 @@ int cellato_server_create(const cellato_server_config* cfg, cellato_server_t* ou
     props.location.type = cudaMemLocationTypeDevice;
     props.location.id = s->dev;
     e = cudaMemPoolCreate(&s->pool, &props);
-    if (e == cudaSuccess) {
-        unsigned long long keep_all = ~0ull;  // freed blocks stay in the pool for the next admissions
-        e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
-    }
+    if (e == cudaSuccess) e = cudaMemPoolCreate(&s->keep_pool, &props);
+    unsigned long long keep_all = ~0ull;  // freed blocks stay in the pools for the next admissions
+    if (e == cudaSuccess) e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+    if (e == cudaSuccess) e = cudaMemPoolSetAttribute(s->keep_pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->main_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming);
     s->slots.resize(s->max_inflight);
@@ -395,8 +407,26 @@ int cellato_server_iterate(cellato_server_t s, int* active) {
         const int rc = harvest_one(s, true);
         if (rc < 0) return -rc;
     }
-    for (long long id : s->sched.admit())
-        if (int rc = materialise(s, id)) return rc;
+    {
+        const std::vector<long long> admitted = s->sched.admit();
+        for (size_t i = 0; i < admitted.size(); ++i) {
+            const int rc = materialise(s, admitted[i]);
+            if (rc == NO_MEMORY) {
+                // back-pressure: this request and the later ones wait, the
+                // cap falls to what is resident; a request that holds the
+                // device alone and still finds no room can never run
+                const req_rec& r = s->recs[admitted[i]];
+                if (i == 0 && s->sched.resident_bytes() == (long long)(2 * (size_t)r.nb * r.stride)) {
+                    s->broken = true;
+                    return fail(CELLATO_ECUDA, "request %lld does not fit in device memory alone", admitted[i]);
+                }
+                s->sched.unadmit(std::vector<long long>(admitted.begin() + i, admitted.end()));
+                ++s->memory_waits;
+                break;
+            }
+            if (rc) return rc;
+        }
+    }
 
     sv::iteration_plan plan = s->sched.plan();
     s->last_active = (long long)plan.active.size();
@@ -611,6 +641,7 @@ int cellato_server_stats_get(cellato_server_t s, cellato_server_stats* st) {
     st->kernel_launches = s->launches;
     st->cell_steps = s->cell_steps;
     st->pool_trims = s->pool_trims;
+    st->memory_waits = s->memory_waits;
     return CELLATO_OK;
 }
 

@@ -157,6 +157,23 @@ public:
         return p;
     }
 
+    // Back-pressure from the device: requests just admitted (in admission
+    // order) that could not get their memory go back to the head of the
+    // waiting queue in the same order, and the cap falls to the bytes still
+    // resident (at least the head request's), so admission waits for resident
+    // requests to finish.
+    void unadmit(const std::vector<long long>& ids) {
+        if (ids.empty()) return;
+        for (auto it = ids.rbegin(); it != ids.rend(); ++it) {
+            request& r = reqs_[*it];
+            r.ph = phase::waiting;
+            resident_bytes_ -= r.bytes;
+            order_.erase(std::find(order_.begin(), order_.end(), *it));
+            waiting_.push_front(*it);
+        }
+        lim_.cap_bytes = std::max(resident_bytes_, reqs_[ids.front()].bytes);
+    }
+
     // Forgets a finished request; returns false when it is unknown or not finished.
     bool release(long long id) {
         auto it = reqs_.find(id);

@@ -25,7 +25,7 @@
 
 // Version of the rule_ops layout; cellato_rule_register refuses a table built
 // against another version.
-#define CELLATO_RULE_OPS_ABI 3
+#define CELLATO_RULE_OPS_ABI 4
 
 namespace cellato::b200 {
 // Single-step kernel choices (cellato_tune::simple_kernel).
@@ -42,9 +42,10 @@ struct cellato_rule_ops_st {
     const char* name;
     int planes;  // needed_bits
     int states;  // number_of_values
-    // one time step t (its parity selects the instantiation) with single-step kernel `variant`
+    // one time step t (its parity selects the instantiation) with single-step kernel `variant`;
+    // words_per_lane: the TMA kernel's words per lane (0: its default)
     cudaError_t (*simple)(int layout, const cellato::b200::plane_set& in, const cellato::b200::plane_set& out, int Xw,
-                          int Y, int t, int variant, cudaStream_t s);
+                          int Y, int t, int variant, int words_per_lane, cudaStream_t s);
     // k fused steps from t0 on a TH-row tile with an HY-row halo, row loop `loop`,
     // V words per lane (a value temporal_v returned)
     cudaError_t (*temporal)(int layout, const cellato::b200::plane_set& in, const cellato::b200::plane_set& out,
@@ -139,17 +140,20 @@ struct rule_kernels {
         return cudaGetLastError();
     }
 
-    // the TMA-fed single-step kernel (rows of a multiple of its strip width)
+    // the TMA-fed single-step kernel (rows of a multiple of its strip width);
+    // V words per lane: the default, or 1, 2 (rules of up to three planes) or 4
+    // (one-plane rules, the 4- and 1-row layouts) when asked for
     template <int LAYOUT>
     static constexpr int TMA_V = tma_default_v<NB, LAYOUT>();
     template <int LAYOUT>
+    static constexpr int TMA_VMAX = NB == 1 && LAYOUT != LAYOUT_TILED8 ? 4 : (NB <= 3 ? 2 : 1);
+    template <int LAYOUT, int V>
     static bool tma_fits(int Xw, int Y) {
-        using G = tma_geom<NB, LAYOUT, TMA_V<LAYOUT>>;
+        using G = tma_geom<NB, LAYOUT, V>;
         return Xw % G::SW == 0 && Y / band_rows<LAYOUT>() >= G::BR;
     }
-    template <int LAYOUT>
+    template <int LAYOUT, int V>
     static cudaError_t simple_tma(const plane_set& in, const plane_set& out, int Xw, int Y, int t, cudaStream_t s) {
-        constexpr int V = TMA_V<LAYOUT>;
         using SM = tma_geom<NB, LAYOUT, V>;
         const int M = Y / band_rows<LAYOUT>();
         tma_maps maps;
@@ -188,8 +192,15 @@ struct rule_kernels {
 
     template <int LAYOUT>
     static cudaError_t simple_layout(const plane_set& in, const plane_set& out, int Xw, int Y, int t, int variant,
-                                     cudaStream_t s) {
-        if (variant == SIMPLE_TMA && tma_fits<LAYOUT>(Xw, Y)) return simple_tma<LAYOUT>(in, out, Xw, Y, t, s);
+                                     int words_per_lane, cudaStream_t s) {
+        if (variant == SIMPLE_TMA) {
+            const int v = words_per_lane ? words_per_lane : TMA_V<LAYOUT>;
+            if (v == 1 && tma_fits<LAYOUT, 1>(Xw, Y)) return simple_tma<LAYOUT, 1>(in, out, Xw, Y, t, s);
+            if constexpr (TMA_VMAX<LAYOUT> >= 2)
+                if (v == 2 && tma_fits<LAYOUT, 2>(Xw, Y)) return simple_tma<LAYOUT, 2>(in, out, Xw, Y, t, s);
+            if constexpr (TMA_VMAX<LAYOUT> >= 4)
+                if (v == 4 && tma_fits<LAYOUT, 4>(Xw, Y)) return simple_tma<LAYOUT, 4>(in, out, Xw, Y, t, s);
+        }
         if constexpr (LAYOUT == LAYOUT_LINEAR) {
             const bool stream_ok = Xw % 4 == 0;
             // default: streaming for rules with two or more planes, whose
@@ -207,11 +218,11 @@ struct rule_kernels {
     }
 
     static cudaError_t simple(int layout, const plane_set& in, const plane_set& out, int Xw, int Y, int t,
-                              int variant, cudaStream_t s) {
+                              int variant, int words_per_lane, cudaStream_t s) {
         switch (layout) {
-            case LAYOUT_LINEAR: return simple_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t, variant, s);
-            case LAYOUT_TILED4: return simple_layout<LAYOUT_TILED4>(in, out, Xw, Y, t, variant, s);
-            case LAYOUT_TILED8: return simple_layout<LAYOUT_TILED8>(in, out, Xw, Y, t, variant, s);
+            case LAYOUT_LINEAR: return simple_layout<LAYOUT_LINEAR>(in, out, Xw, Y, t, variant, words_per_lane, s);
+            case LAYOUT_TILED4: return simple_layout<LAYOUT_TILED4>(in, out, Xw, Y, t, variant, words_per_lane, s);
+            case LAYOUT_TILED8: return simple_layout<LAYOUT_TILED8>(in, out, Xw, Y, t, variant, words_per_lane, s);
         }
         return cudaErrorInvalidValue;
     }

@@ -339,10 +339,10 @@ def describe_choice(c: dict) -> str:
     """The autotuner's choice as text: mode, k, tile rows (0 = default), row
     loop, tile width and, when tuned, the word size."""
     w = f" W{c['word_bits']}" if "word_bits" in c else ""
+    width = {0: "default", 1: "1", 2: "2", 4: "4"}[c.get("width", 0)]
     if c["mode"] != "temporal":
-        return c["mode"] + w
+        return c["mode"] + (f" words_per_lane={width}" if c.get("width", 0) else "") + w
     loop = {0: "default", 1: "row-by-row", 2: "hoisted", 3: "paired"}[c.get("loop", 0)]
-    width = {0: "default", 1: "1", 2: "2"}[c.get("width", 0)]
     return f"temporal k={c['k']} tile_rows={c.get('tile_rows', 0)} loop={loop} words_per_lane={width}{w}"
 
 
@@ -545,23 +545,33 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
 
     peaks = measured_peaks()
     # ---- the best single-step kernel of each automaton against the HBM roofline
-    # (one step per launch: read and write every plane once)
+    # (one step per launch: read and write every plane once), the word size
+    # tuned for it as the workload leaves it open
     single = {}
     for a, g in grids.items():
-        c1 = autotune.tune(g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y,
-                           candidates=autotune.SINGLE_STEP_CANDIDATES, use_cache=False)
-        g["a"].buf.copy_(g["init"].buf)
+        cells = torch.from_numpy(inputs.workload_grid(a, X, Y, SEED + rank)).to(dev)
+        c1 = autotune.tune_word_bits(g["rule"], LAYOUT, cells, X, Y, word_bits=WORD_CHOICES[LAYOUT],
+                                     candidates=autotune.SINGLE_STEP_CANDIDATES, use_cache=False)
+        W1 = c1["word_bits"]
+        if W1 == g["W"]:
+            pa, pb = g["a"], g["b"]
+            pa.buf.copy_(g["init"].buf)
+        else:
+            pa, pb = DevicePlanes(g["nb"], X, Y, dev), DevicePlanes(g["nb"], X, Y, dev)
+            pa.pack_from(cells, LAYOUT, W1, sp)
+        del cells
         n1 = 16
-        autotune.run(c1, g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, 0, 2, sp)
+        autotune.run(c1, g["rule"], LAYOUT, W1, pa.ptrs, pb.ptrs, X, Y, 0, 2, sp)
         e0.record(stream)
-        autotune.run(c1, g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, 0, n1, sp)
+        autotune.run(c1, g["rule"], LAYOUT, W1, pa.ptrs, pb.ptrs, X, Y, 0, n1, sp)
         e1.record(stream)
         torch.cuda.synchronize()
         ms1 = e0.elapsed_time(e1) / n1
         gbs = 2 * g["nb"] * g["init"].plane_bytes / (ms1 * 1e-3) / 1e9
-        single[a] = {"kernel": describe_choice(c1), "ms_per_step": round(ms1, 4), "achieved_gbs": round(gbs, 1),
-                     "frac": round(gbs / peaks["hbm_gbs"], 4),
+        single[a] = {"kernel": describe_choice(c1), "word_bits": W1, "ms_per_step": round(ms1, 4),
+                     "achieved_gbs": round(gbs, 1), "frac": round(gbs / peaks["hbm_gbs"], 4),
                      "gcups": round(X * Y / (ms1 * 1e-3) / 1e9, 1)}
+        del pa, pb
         g["a"].buf.copy_(g["init"].buf)
     torch.cuda.synchronize()
 
@@ -949,7 +959,8 @@ def served_arm(args, rank: int, world: int):
         "served_over_per_grid": round(value / world / base["gcups"], 2) if base else None,
         "sample_bit_exact": f"{sample_ok}/{len(sample)}",
         "server": {"iterations": stats["iterations"], "kernel_launches": stats["kernel_launches"],
-                   "pool_trims": stats["pool_trims"]},
+                   "pool_trims": stats["pool_trims"], "memory_waits": stats["memory_waits"],
+                   "hbm_cap_bytes_at_end": stats["hbm_cap_bytes"]},
         "e2e": {"value": round(value, 1), "unit": "GCUPS", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": 128 * n,
                 "note": "requests enter through the server's C ABI as seeds; results leave as 16 tile sums each"},

@@ -91,12 +91,17 @@ typedef struct cellato_rule_ops_st cellato_rule_ops;
 typedef struct {
     int simple_kernel;   /* single-step kernel: 0 automatic, 1 register bands, 2 bulk-copy streaming (linear
                             layout, rows of 16-byte multiples; others use 1), 3 TMA-fed shared-memory tiles
-                            (rows of a multiple of 4096 cells; others use 1) */
+                            (rows of a multiple of its strip, 4096 cells at one word per lane and 8192 at
+                            two or four; others use 1) */
     int row_loop;        /* temporal row loop: 0 automatic, 1 row by row, 2 the input rows of each three-row
                             trip read before its in-place writes, 3 as 2 with two steps per sweep of the
                             tile (an odd last step runs alone) */
-    int words_per_lane;  /* temporal tile width: 0 the rule's default (2 for one-plane rules, else 1), 1, or 2
-                            (rules of up to three planes; others use 1); the tile is 32 x this many words */
+    int words_per_lane;  /* words per lane, 0 the default, else 1, 2 or 4.  Temporal tile width: default 2 for
+                            one-plane rules, else 1; 2 and 4 only for rules of up to three planes (others use
+                            1, and 4 means 2); the tile is 32 x this many words.  TMA single-step kernel: 2 for
+                            rules of up to three planes, 4 for one-plane rules outside the 8-row tiled
+                            layout; a width the rule or the grid does not allow falls back to the register
+                            kernel */
     int tile_rows;       /* temporal tile rows including both k-row halos; 0 the library's default */
 } cellato_tune;
 
@@ -170,8 +175,8 @@ int cellato_unpack_cells(int layout, int word_bits, int nb, const void* const* p
  * process_grid_kernel_simple :20-39): `steps` single-step launches, ping-pong
  * between planes_a (input) and planes_b.  *result_in_b is set to 1 when the
  * final state is in planes_b (odd number of launches), else 0.  tune: NULL or
- * its simple_kernel field (the other fields are ignored).  Nothing is
- * allocated; planes_a and planes_b must not overlap. */
+ * its simple_kernel and words_per_lane fields (the others are ignored).
+ * Nothing is allocated; planes_a and planes_b must not overlap. */
 int cellato_run_simple(int rule, int layout, int word_bits, void* const* planes_a, void* const* planes_b,
                        int x_cells, int y_cells, int t0, int steps, const cellato_tune* tune,
                        cellato_stream_t stream, int* result_in_b);
@@ -382,6 +387,9 @@ typedef struct {
     double cell_steps;                /* cell updates enqueued since creation */
     long long pool_trims;             /* times a plane allocation found the pool fragmented: issued frees
                                          were completed, unused blocks returned, the allocation retried */
+    long long memory_waits;           /* times admitted requests found no device memory even then: they
+                                         went back to the head of the queue and the cap fell to the bytes
+                                         resident (hbm_cap_bytes shows the current cap) */
 } cellato_server_stats;
 
 int cellato_server_create(const cellato_server_config* config, cellato_server_t* out);

@@ -35,7 +35,7 @@ def main() -> None:
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--loop", type=int, default=0, help="temporal row loop (cellato_tune.row_loop)")
-    ap.add_argument("--width", type=int, default=0, help="temporal words per lane (cellato_tune.words_per_lane)")
+    ap.add_argument("--width", type=int, default=0, help="words per lane (cellato_tune.words_per_lane)")
     ap.add_argument("--simple-kernel", type=int, default=0, help="single-step kernel (cellato_tune.simple_kernel)")
     ap.add_argument("--launches", type=int, default=3)
     ap.add_argument("--grids", type=int, default=512, help="batch: grids in the batch (the batched workload's "
@@ -62,7 +62,8 @@ def main() -> None:
 
     def launch(n):
         if a.mode == "simple":
-            return lib.run_simple(r, layout, a.word_bits, pa.ptrs, pb.ptrs, X, Y, 0, n, simple_kernel=a.simple_kernel)
+            return lib.run_simple(r, layout, a.word_bits, pa.ptrs, pb.ptrs, X, Y, 0, n, simple_kernel=a.simple_kernel,
+                                  words_per_lane=a.width)
         return lib.run_temporal(r, layout, a.word_bits, pa.ptrs, pb.ptrs, X, Y, 0, n * k, k, a.tile_rows,
                                 row_loop=a.loop, words_per_lane=a.width)
 

@@ -109,23 +109,33 @@ def test_config3_size_temporal_equals_single_step(cuda, rule):
 
 
 @pytest.mark.parametrize("rule,layout,S,W", [("wire", 1, 16384, 32), ("excitable", 1, 16384, 64),
-                                             ("cyclic", 0, 32768, 64), ("fluid", 0, 32768, 64)])
+                                             ("cyclic", 0, 32768, 64), ("fluid", 0, 32768, 64),
+                                             ("game-of-life", 0, 32768, 64), ("wire", 0, 32768, 64)])
 def test_tma_single_step_equals_register_kernel(cuda, rule, layout, S, W):
-    """The TMA-fed single-step kernel against the register-band kernel at the
-    workloads' full sizes, both word sizes of the tiled layout."""
+    """The TMA-fed single-step kernel, at its default and every words-per-lane
+    width the rule allows, against the register-band kernel at the workloads'
+    full sizes, both word sizes of the tiled layout."""
     import torch
     from cellato_b200.device import DevicePlanes
     r = lib.rule_id(rule)
     nb = inputs.PLANES[r]
     steps = 7
-    outs = []
-    for kernel in (1, 3):
+
+    def run_kernel(kernel, width):
         a, b = DevicePlanes(nb, S, S), DevicePlanes(nb, S, S)
         lib.fill_random(layout, W, nb, a.ptrs, S, S, 9, inputs.thresholds(inputs.REFERENCE_DENSITY[rule]))
-        in_b = lib.run_simple(r, layout, W, a.ptrs, b.ptrs, S, S, 0, steps, simple_kernel=kernel)
-        outs.append(b if in_b else a)
-        del a, b
-    assert diff(nb, outs[0], outs[1]) == 0
+        in_b = lib.run_simple(r, layout, W, a.ptrs, b.ptrs, S, S, 0, steps, simple_kernel=kernel,
+                              words_per_lane=width)
+        return b if in_b else a
+
+    ref = run_kernel(1, 0)
+    for width in (0, 1, 2, 4):
+        if (width == 2 and nb > 3) or (width == 4 and nb > 1):
+            continue
+        got = run_kernel(3, width)
+        assert diff(nb, ref, got) == 0, width
+        del got
+        torch.cuda.empty_cache()
     assert lib.device_wait_timeouts() == 0
-    del outs
+    del ref
     torch.cuda.empty_cache()

@@ -25,7 +25,8 @@ def run_gpu(oracle, rule, layout, W, cells, steps, mode="simple", k=1, t0=0, til
     b = DevicePlanes(nb, X, Y)
     a.upload(oracle.pack(layout, W, nb, cells))
     if mode == "simple":
-        in_b = lib.run_simple(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps, simple_kernel=simple_kernel)
+        in_b = lib.run_simple(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps, simple_kernel=simple_kernel,
+                              words_per_lane=words_per_lane)
     else:
         in_b = lib.run_temporal(rule, layout, W, a.ptrs, b.ptrs, X, Y, t0, steps, k, tile_rows,
                                 row_loop=row_loop, words_per_lane=words_per_lane)
@@ -158,15 +159,21 @@ def test_streaming_kernel_shapes_and_no_wait_timeouts(cuda, oracle):
 
 
 @pytest.mark.parametrize("layout,W", LAYOUTS)
-def test_tma_single_step_kernel(cuda, oracle, layout, W):
-    """The TMA-fed single-step kernel (cellato_tune.simple_kernel = 3, rows of
-    a multiple of 4096 cells): every rule, one and two strips per row, heights
-    from one stage to several CTAs per strip, wrapped halos, odd step offsets."""
-    rng = np.random.default_rng(31 + layout + W)
+@pytest.mark.parametrize("width", [0, 1, 2, 4])
+def test_tma_single_step_kernel(cuda, oracle, layout, W, width):
+    """The TMA-fed single-step kernel (cellato_tune.simple_kernel = 3) at its
+    default and every words-per-lane width a rule allows (strips of 4096 cells
+    at one word per lane, 8192 at two or four; narrower rows fall back to the
+    register kernel): every rule, one and two strips per row, heights from one
+    stage to several CTAs per strip, wrapped halos, odd step offsets."""
+    rng = np.random.default_rng(31 + layout + W + width)
     for r in range(10):
-        for X, Y in [(4096, 96), (8192, 40), (4096, 264)]:
+        nb = inputs.PLANES[r]
+        if (width == 2 and nb > 3) or (width == 4 and nb > 1):
+            continue
+        for X, Y in [(4096, 96), (8192, 40), (4096, 264), (16384, 24), (8192, 136)]:
             cells = rng.integers(0, inputs.STATES[r], size=(Y, X), dtype=np.uint8)
             want = oracle.run(r, cells, 5, t0=3)
-            got = run_gpu(oracle, r, layout, W, cells, 5, t0=3, simple_kernel=3)
-            assert np.array_equal(got, want), (RULES[r], X, Y, layout, W)
+            got = run_gpu(oracle, r, layout, W, cells, 5, t0=3, simple_kernel=3, words_per_lane=width)
+            assert np.array_equal(got, want), (RULES[r], X, Y, layout, W, width)
     assert lib.device_wait_timeouts() == 0
