@@ -963,6 +963,57 @@ CB_HD constexpr word var_pattern(int j, int half) {
     return j < 5 ? pat[j] : (half ? ~word(0) : word(0));
 }
 
+// Counts of a fixed state enter a synthesised network unfinished: the network
+// receives the carry-save halves of the count, and the last additions become
+// part of the network's own LOP3s.
+//   Moore: low = a.s3 + b.s3 + m.s2 and high = a.c3 + b.c3 + m.c2 (each 0..3,
+//     two planes: xor3 and maj3), count = low + 2 high -- four LOP3s where
+//     the binary count (lower<count_neighbors<...>> above) takes eight;
+//   von Neumann: low = u + d + m.s2 (xor3, maj3) and m.c2, count = low +
+//     2 m.c2 -- two LOP3s where the binary count takes four.
+// The symbolic context adds the halves back into the binary count on
+// truth-table patterns, so the rule sees the same count.
+template <class S>
+struct packed_count : std::false_type {};
+template <auto V>
+struct packed_count<ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>> : std::true_type {
+    CB_HD static constexpr planes<4> binary(const word* x) {  // x: low0, low1, high0, high1
+        const word c1 = x[1] & x[2];
+        return planes<4>{{x[0], word(x[1] ^ x[2]), word(x[3] ^ c1), word(x[3] & c1)}};
+    }
+};
+template <auto V>
+struct packed_count<ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>> : std::true_type {
+    CB_HD static constexpr planes<3> binary(const word* x) {  // x: low0, low1, m.c2
+        return planes<3>{{x[0], word(x[1] ^ x[2]), word(x[1] & x[2])}};
+    }
+};
+
+template <class Dict, class Targets, class S>
+struct packed_signal;
+template <class Dict, class Targets, auto V>
+struct packed_signal<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>> {
+    static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
+    template <class C>
+    CB_HD static planes<4> eval(const C& c) {
+        const count_cache& a = c.up.cc[slot];
+        const count_cache& b = c.dn.cc[slot];
+        const count_cache& m = c.mid.cc[slot];
+        return planes<4>{{xor3(a.s3, b.s3, m.s2), maj3(a.s3, b.s3, m.s2), xor3(a.c3, b.c3, m.c2),
+                          maj3(a.c3, b.c3, m.c2)}};
+    }
+};
+template <class Dict, class Targets, auto V>
+struct packed_signal<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::von_neumann_4_neighbors>> {
+    static constexpr int slot = iindex<Targets, Dict::state_to_index(V)>::value;
+    template <class C>
+    CB_HD static planes<3> eval(const C& c) {
+        const word u = c.up.cc[slot].P[1], d = c.dn.cc[slot].P[1];
+        const count_cache& m = c.mid.cc[slot];
+        return planes<3>{{xor3(u, d, m.s2), maj3(u, d, m.s2), m.c2}};
+    }
+};
+
 // Symbolic evaluation context: signal S yields planes of variable patterns.
 template <class Dict, class Signals, int TP, int HALF>
 struct sym_ctx {
@@ -972,8 +1023,12 @@ struct sym_ctx {
     constexpr auto sig() const {
         constexpr int off = signal_layout<Dict, Signals>::template offset<S>();
         constexpr int w = signal_width<Dict, S>::value;
-        if constexpr (w == 1 && !std::is_same_v<S, ast::neighbor_at<0, 0>> &&
-                      !std::is_same_v<S, ast::margolus_180_neighbor>) {
+        if constexpr (packed_count<S>::value) {
+            word x[w] = {};
+            for (int i = 0; i < w; ++i) x[i] = var_pattern(off + i, HALF);
+            return packed_count<S>::binary(x);
+        } else if constexpr (w == 1 && !std::is_same_v<S, ast::neighbor_at<0, 0>> &&
+                             !std::is_same_v<S, ast::margolus_180_neighbor>) {
             return var_pattern(off, HALF);  // a condition
         } else {
             planes<w> r{};
@@ -1004,11 +1059,11 @@ struct lop_net {
 };
 
 constexpr tt_t tt_mask(int n) { return n >= 6 ? ~tt_t(0) : ((tt_t(1) << (1 << n)) - 1); }
+// bit m of variable j's table = bit j of m, for up to six variables
 constexpr tt_t tt_var(int j, int n) {
-    tt_t p = 0;
-    for (int m = 0; m < (1 << n); ++m)
-        if ((m >> j) & 1) p |= tt_t(1) << m;
-    return p;
+    constexpr tt_t pat[6] = {0xAAAAAAAAAAAAAAAAull, 0xCCCCCCCCCCCCCCCCull, 0xF0F0F0F0F0F0F0F0ull,
+                             0xFF00FF00FF00FF00ull, 0xFFFF0000FFFF0000ull, 0xFFFFFFFF00000000ull};
+    return pat[j] & tt_mask(n);
 }
 constexpr tt_t tt_cof(tt_t t, int v, int val, int n) {
     const tt_t pv = tt_var(v, n);
@@ -1257,12 +1312,20 @@ struct rule_net {
             ...);
     }
 
+    template <class S, class C>
+    CB_HD static auto signal_value(const C& c) {
+        if constexpr (packed_count<S>::value)
+            return packed_signal<Dict, targets, S>::eval(c);  // the network finishes the count
+        else
+            return as_planes(ev<Dict, targets, S>(c));
+    }
+
     template <int TP, class C, class... Ss>
     CB_HD static void fill_signals(const C& c, word* v, tlist<Ss...>) {
         using L = signal_layout<Dict, tlist<Ss...>>;
         (
             [&] {
-                const auto s = as_planes(ev<Dict, targets, Ss>(c));
+                const auto s = signal_value<Ss>(c);
                 constexpr int off = L::template offset<Ss>();
 #pragma unroll
                 for (int i = 0; i < decltype(s)::width; ++i) v[off + i] = s.p[i];
