@@ -68,10 +68,10 @@ CPU_SAMPLE_SIZE = 2048
 # sources it was captured from (kernel_source_hash); an entry whose hash no
 # longer matches the sources is reported as stale and not used.
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 12, 16384): (87.34e6, "profiles/temporal_kernel_dram_alu_captures.md", "6e7165e6054cc5cd"),
-    ("excitable", "temporal", 16, 16384): (152.93e6, "profiles/temporal_kernel_dram_alu_captures.md", "4bd271d08768106a"),
-    ("cyclic", "temporal", 8, 32768): (1293.69e6, "profiles/temporal_kernel_dram_alu_captures.md", "4d616ed2498b26a1"),
-    ("fluid", "temporal", 16, 32768): (1025.51e6, "profiles/temporal_kernel_dram_alu_captures.md", "501b6d5b0c8e008b"),
+    ("wire", "temporal", 16, 16384): (87.22e6, "profiles/temporal_kernel_dram_alu_captures.md", "ae675c8f429699d4"),
+    ("excitable", "temporal", 16, 16384): (151.67e6, "profiles/temporal_kernel_dram_alu_captures.md", "f92a9f9077491d6a"),
+    ("cyclic", "temporal", 8, 32768): (1295.05e6, "profiles/temporal_kernel_dram_alu_captures.md", "5ea40358ff40fd7f"),
+    ("fluid", "temporal", 16, 32768): (1030.94e6, "profiles/temporal_kernel_dram_alu_captures.md", "5ecc24a66b672e76"),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
@@ -81,10 +81,10 @@ MEASURED_TRAFFIC = {
 # Each configuration is timed live and set against the ALU pipe's measured rate
 # (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 32, 12, 0, 3, 1, 16384): (98888256, "profiles/temporal_kernel_dram_alu_captures.md", "6e7165e6054cc5cd"),
-    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (72008352, "profiles/temporal_kernel_dram_alu_captures.md", "4bd271d08768106a"),
-    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "4d616ed2498b26a1"),
-    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "501b6d5b0c8e008b"),
+    ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "ae675c8f429699d4"),
+    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (72008352, "profiles/temporal_kernel_dram_alu_captures.md", "f92a9f9077491d6a"),
+    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "5ea40358ff40fd7f"),
+    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "5ecc24a66b672e76"),
 }
 
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
