@@ -383,10 +383,27 @@ template <class T, auto Z>
 struct uses_sums<ast::greater_than<ast::count_neighbors<T, ast::von_neumann_4_neighbors>, ast::constant<Z>>, void>
     : std::bool_constant<Z != 0 || uses_sums<T>::value> {};
 
+// uses_any<E>: E tests "any Moore neighbour is S" (count > 0) for a fixed S,
+// which reads the per-row ORs of the predicates.
+template <class E, class = void>
+struct uses_any : std::false_type {};
+template <class V, int b>
+struct uses_any<ast::has_bit_set<V, b>, void> : uses_any<V> {};
+template <template <class...> class N, class... Ch>
+struct uses_any<N<Ch...>, std::enable_if_t<!is_count_test<N<Ch...>>::value>>
+    : std::bool_constant<(uses_any<Ch>::value || ...)> {};
+template <class T, auto Z>
+struct uses_any<ast::greater_than<ast::count_neighbors<T, ast::moore_8_neighbors>, ast::constant<Z>>, void>
+    : std::bool_constant<(Z == 0 && is_state_const<T>::value) || uses_any<T>::value> {};
+template <class T, auto Z>
+struct uses_any<ast::greater_than<ast::count_neighbors<T, ast::von_neumann_4_neighbors>, ast::constant<Z>>, void>
+    : uses_any<T> {};
+
 // ------------------------------------------------------------ per-row cache
 // Predicate "cell == S" at dx = -1, 0, +1 and its partial sums.
 struct count_cache {
     word P[3];   // P[dx + 1]
+    word o2, o3; // P[0] | P[2], P[0] | P[1] | P[2]  (any-neighbour tests)
     word s3, c3; // P[0] + P[1] + P[2]  (sum, carry)
     word s2, c2; // P[0] + P[2]
 };
@@ -415,7 +432,7 @@ CB_HD pred_set<ilist<S...>> preds_of_impl(const word* C, ilist<S...>) {
 // Builds a row's features for one word from its own planes (C), the words to
 // its left and right (L, R: only bit 31 / bit 0 matter, read only when SHIFT)
 // and the count-target predicates of the three words.
-template <int NB, class Targets, bool SHIFT, bool SUMS>
+template <int NB, class Targets, bool SHIFT, bool SUMS, bool ANY = false>
 CB_HD row_feat<NB, Targets> make_row_feat(const word* C, const word* L, const word* R, const pred_set<Targets>& pc,
                                           const pred_set<Targets>& pl, const pred_set<Targets>& pr) {
     row_feat<NB, Targets> f;
@@ -438,6 +455,10 @@ CB_HD row_feat<NB, Targets> make_row_feat(const word* C, const word* L, const wo
             c.c3 = maj3(c.P[0], c.P[1], c.P[2]);
             c.s2 = c.P[0] ^ c.P[2];
             c.c2 = c.P[0] & c.P[2];
+        }
+        if constexpr (ANY) {
+            c.o2 = c.P[0] | c.P[2];
+            c.o3 = c.o2 | c.P[1];
         }
     }
     return f;
@@ -705,10 +726,9 @@ struct lower<Dict, Targets,
     template <class C>
     CB_HD static constexpr word eval(const C& c) {
         if constexpr (Z == 0) {
-            const count_cache& a = c.up.cc[slot];
-            const count_cache& b = c.dn.cc[slot];
-            const count_cache& m = c.mid.cc[slot];
-            return a.P[0] | a.P[1] | a.P[2] | b.P[0] | b.P[1] | b.P[2] | m.P[0] | m.P[2];
+            // the rows above and below contribute their 3-cell ORs, the own
+            // row its 2-cell OR (row features built with uses_any)
+            return c.up.cc[slot].o3 | c.dn.cc[slot].o3 | c.mid.cc[slot].o2;
         } else {
             // through ev, so that a symbolic context substitutes the count signal
             return gt(ev<Dict, Targets, ast::count_neighbors<ast::state_constant<V>, ast::moore_8_neighbors>>(c),
@@ -1257,13 +1277,14 @@ struct rule_net {
     using preds_t = pred_set<targets>;
     static constexpr bool need_shift = uses_shift<Rule>::value;
     static constexpr bool need_sums = uses_sums<Rule>::value;
+    static constexpr bool need_any = uses_any<Rule>::value;
 
     CB_HD static preds_t preds(const word* C) { return preds_of_impl<NB>(C, targets{}); }
 
     // features of one word given its neighbours' predicates
     CB_HD static feat make(const word* C, const word* L, const word* R, const preds_t& pc, const preds_t& pl,
                            const preds_t& pr) {
-        return make_row_feat<NB, targets, need_shift, need_sums>(C, L, R, pc, pl, pr);
+        return make_row_feat<NB, targets, need_shift, need_sums, need_any>(C, L, R, pc, pl, pr);
     }
 
     // features of one word from its own and its two neighbour words
