@@ -68,10 +68,10 @@ CPU_SAMPLE_SIZE = 2048
 # sources it was captured from (kernel_source_hash); an entry whose hash no
 # longer matches the sources is reported as stale and not used.
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 16, 16384): (87.22e6, "profiles/temporal_kernel_dram_alu_captures.md", "ae675c8f429699d4"),
-    ("excitable", "temporal", 16, 16384): (151.67e6, "profiles/temporal_kernel_dram_alu_captures.md", "f92a9f9077491d6a"),
-    ("cyclic", "temporal", 8, 32768): (1295.05e6, "profiles/temporal_kernel_dram_alu_captures.md", "5ea40358ff40fd7f"),
-    ("fluid", "temporal", 16, 32768): (1030.94e6, "profiles/temporal_kernel_dram_alu_captures.md", "5ecc24a66b672e76"),
+    ("wire", "temporal", 16, 16384): (86.71e6, "profiles/temporal_kernel_dram_alu_captures.md", "236c7ee2e6bf1248"),
+    ("excitable", "temporal", 16, 16384): (151.75e6, "profiles/temporal_kernel_dram_alu_captures.md", "857178ef3695312b"),
+    ("cyclic", "temporal", 8, 32768): (1292.52e6, "profiles/temporal_kernel_dram_alu_captures.md", "05533d7c3cdc1366"),
+    ("fluid", "temporal", 16, 32768): (1025.78e6, "profiles/temporal_kernel_dram_alu_captures.md", "2481b8a1356b1f6f"),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
@@ -81,10 +81,10 @@ MEASURED_TRAFFIC = {
 # Each configuration is timed live and set against the ALU pipe's measured rate
 # (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "ae675c8f429699d4"),
-    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (72008352, "profiles/temporal_kernel_dram_alu_captures.md", "f92a9f9077491d6a"),
-    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "5ea40358ff40fd7f"),
-    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "5ecc24a66b672e76"),
+    ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "236c7ee2e6bf1248"),
+    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (71637912, "profiles/temporal_kernel_dram_alu_captures.md", "857178ef3695312b"),
+    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "05533d7c3cdc1366"),
+    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "2481b8a1356b1f6f"),
 }
 
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
