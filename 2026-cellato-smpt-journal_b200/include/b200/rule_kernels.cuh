@@ -97,8 +97,11 @@ struct rule_kernels {
     // which wastes less on the narrow grids of a batch, and its register use
     // leaves room for three CTAs per SM.
     static constexpr int BATCH_V = 1;
-    // ... and two steps per sweep of a tile (row loop 3)
-    static constexpr bool BATCH_PAIR = true;
+    // ... and two steps per sweep of a tile (row loop 3) for rules of up to
+    // three planes; with four or five planes the second step's features cost
+    // registers that leave one or two CTAs per SM (cyclic: 177 registers, one
+    // CTA per SM, 12.5% warps active in a 1024-grid batch on B200)
+    static constexpr bool BATCH_PAIR = NB <= 3;
     static constexpr int TEMPORAL_WARPS = 8;
 
     template <int LAYOUT, int V>

@@ -52,16 +52,17 @@ constexpr unsigned TMA_WAIT_LIMIT = 1u << 22;
 constexpr int TMA_STAGE_BUDGET = 8 * 1024;  // bytes of strip data per stage (all planes)
 
 // Default words per lane of the TMA step kernel for a rule of NB planes in a
-// layout: 2 for rules of up to three planes, else 1; and 1 in the 8-row tiled
-// layout, whose eight rows per word already give each lane enough independent
-// work.  Measured on B200 against the other widths: two words there cost
-// registers and occupancy (WireWorld 0.50 against 0.55 and Greenberg-Hastings
-// 0.50 against 0.68 of the HBM peak at 16384^2), and four words per lane for
-// Game of Life on the linear layout reached 0.57 of the peak at 32768^2
-// against 0.61 with two.  Callers may ask for another width per call.
+// layout: 4 for one-plane rules, 2 for two or three planes, else 1; and 1 in
+// the 8-row tiled layout, whose eight rows per word already give each lane
+// enough independent work.  Measured on B200 (fractions of the HBM peak): Game
+// of Life on the linear layout at 32768^2, 0.65 at four words per lane against
+// 0.60 at two and 0.49 at one; WireWorld 0.62 (tiled W64) and 0.79 (linear)
+// at its defaults; two words per lane in the 8-row layout cost registers and
+// occupancy (Greenberg-Hastings 0.52 against 0.69).  Callers may ask for
+// another width per call.
 template <int NB, int LAYOUT>
 constexpr int tma_default_v() {
-    return LAYOUT == LAYOUT_TILED8 ? 1 : (NB <= 3 ? 2 : 1);
+    return LAYOUT == LAYOUT_TILED8 ? 1 : (NB == 1 ? 4 : (NB <= 3 ? 2 : 1));
 }
 
 // Geometry and shared-memory layout of the kernel for (NB, LAYOUT, V).
