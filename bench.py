@@ -68,10 +68,10 @@ CPU_SAMPLE_SIZE = 2048
 # sources it was captured from (kernel_source_hash); an entry whose hash no
 # longer matches the sources is reported as stale and not used.
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 16, 16384): (86.71e6, "profiles/temporal_kernel_dram_alu_captures.md", "236c7ee2e6bf1248"),
-    ("excitable", "temporal", 16, 16384): (151.75e6, "profiles/temporal_kernel_dram_alu_captures.md", "857178ef3695312b"),
-    ("cyclic", "temporal", 8, 32768): (1292.52e6, "profiles/temporal_kernel_dram_alu_captures.md", "05533d7c3cdc1366"),
-    ("fluid", "temporal", 16, 32768): (1025.78e6, "profiles/temporal_kernel_dram_alu_captures.md", "2481b8a1356b1f6f"),
+    ("wire", "temporal", 16, 16384): (86.88e6, "profiles/temporal_kernel_dram_alu_captures.md", "8b09bac81d9f47a3"),
+    ("excitable", "temporal", 16, 16384): (152.15e6, "profiles/temporal_kernel_dram_alu_captures.md", "01d9d66fd15fd82b"),
+    ("cyclic", "temporal", 8, 32768): (1293.26e6, "profiles/temporal_kernel_dram_alu_captures.md", "de7c1cb4beff04ff"),
+    ("fluid", "temporal", 16, 32768): (1025.61e6, "profiles/temporal_kernel_dram_alu_captures.md", "7f66e007783f5d50"),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
@@ -81,10 +81,10 @@ MEASURED_TRAFFIC = {
 # Each configuration is timed live and set against the ALU pipe's measured rate
 # (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "236c7ee2e6bf1248"),
-    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (71637912, "profiles/temporal_kernel_dram_alu_captures.md", "857178ef3695312b"),
-    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "05533d7c3cdc1366"),
-    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "2481b8a1356b1f6f"),
+    ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "8b09bac81d9f47a3"),
+    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (71637912, "profiles/temporal_kernel_dram_alu_captures.md", "01d9d66fd15fd82b"),
+    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "de7c1cb4beff04ff"),
+    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "7f66e007783f5d50"),
 }
 
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
@@ -321,8 +321,9 @@ def reference_arm(args, rank: int, world: int):
 
 
 def parse_choices(text: str) -> dict:
-    """--choice wire=temporal:8:128:1,excitable=temporal:16:0:2:1 (mode:k:tile_rows:loop:words_per_lane)
-    or <automaton>=simple_register / simple_stream: pins the traverser per automaton."""
+    """--choice wire=temporal:8:128:1,excitable=temporal:16:0:3:1:32
+    (mode:k:tile_rows:loop:words_per_lane[:word size]) or <automaton>=simple_register /
+    simple_stream: pins the traverser (and the word size) per automaton."""
     out = {}
     for item in filter(None, (text or "").split(",")):
         name, spec = item.split("=")
@@ -330,6 +331,8 @@ def parse_choices(text: str) -> dict:
         if f[0] == "temporal":
             out[name] = {"mode": "temporal", "k": int(f[1]), "tile_rows": int(f[2]) if len(f) > 2 else 0,
                          "loop": int(f[3]) if len(f) > 3 else 0, "width": int(f[4]) if len(f) > 4 else 0}
+            if len(f) > 5:
+                out[name]["word_bits"] = int(f[5])
         else:
             out[name] = {"mode": f[0], "k": 1, "tile_rows": 0}
     return out
@@ -385,7 +388,7 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
         nb = inputs.PLANES[r]
         cells = torch.from_numpy(inputs.workload_grid(a, X, Y, SEED + rank)).to(dev)
         if a in pinned:
-            choice = dict(pinned[a], word_bits=WORD_BITS)
+            choice = dict(pinned[a], word_bits=pinned[a].get("word_bits", WORD_BITS))
         else:
             choice = autotune.tune_word_bits(r, LAYOUT, cells, X, Y, word_bits=WORD_CHOICES[LAYOUT],
                                              candidates=cands, use_cache=False)
