@@ -93,10 +93,13 @@ struct rule_kernels {
     static_assert(NB <= MAX_PLANES, "too many planes");
     static constexpr int SIMPLE_WARPS = 4;
     static constexpr int TEMPORAL_V = NB <= 3 ? 2 : 1;
-    // The batched kernel runs one word per lane: its tiles are 32 words wide,
-    // which wastes less on the narrow grids of a batch, and its register use
-    // leaves room for three CTAs per SM.
-    static constexpr int BATCH_V = 1;
+    // The batched kernel runs one word per lane for rules of two or more
+    // planes: its tiles are 32 words wide, which wastes less on the narrow
+    // grids of a batch, and its register use leaves room for three CTAs per
+    // SM.  One-plane rules take two words per lane: with one word a lane has
+    // too little independent work (Game of Life, maze and critters ran at
+    // 0.31-0.48 of their single-grid rate in a 1024-grid batch on B200).
+    static constexpr int BATCH_V = NB == 1 ? 2 : 1;
     // ... and two steps per sweep of a tile (row loop 3) for rules of up to
     // three planes; with four or five planes the second step's features cost
     // registers that leave one or two CTAs per SM (cyclic: 177 registers, one

@@ -89,14 +89,15 @@ def test_noalloc_rejects_batches_beyond_its_limits(cuda):
     # more grids than CELLATO_NOALLOC_MAX_GRIDS (the count is checked first)
     assert _call([(0, 64, 8, 1, [16], [32])] * 1025) == lib.EINVAL
     assert b"no-allocation limit" in L.cellato_last_error()
-    # under the grid limit but over CELLATO_NOALLOC_MAX_ITEMS work items:
-    # a 4096^2 grid in tiles of 30 words x 128 rows (k = 2) is 160 tiles a
-    # round, 500 rounds = 80,000 items; nothing may run
+    # under the grid limit but over CELLATO_NOALLOC_MAX_ITEMS work items: a
+    # 4096^2 WireWorld grid (two planes: tiles of 30 words x 128 rows, k = 2)
+    # is 160 tiles a round, 500 rounds = 80,000 items; nothing may run
     X = Y = 4096
-    a, b = DevicePlanes(1, X, Y), DevicePlanes(1, X, Y)
+    wire = lib.rule_id("wire")
+    a, b = DevicePlanes(2, X, Y), DevicePlanes(2, X, Y)
     a.buf.fill_(0x5A)
     torch.cuda.synchronize()
-    rc = _call([(0, X, Y, 1000, a.ptrs, b.ptrs)], {0: 2})
+    rc = _call([(wire, X, Y, 1000, a.ptrs, b.ptrs)], {wire: 2})
     torch.cuda.synchronize()
     assert rc == lib.EINVAL
     assert b"no-allocation limit" in L.cellato_last_error()
