@@ -68,10 +68,10 @@ CPU_SAMPLE_SIZE = 2048
 # sources it was captured from (kernel_source_hash); an entry whose hash no
 # longer matches the sources is reported as stale and not used.
 MEASURED_TRAFFIC = {
-    ("wire", "temporal", 16, 16384): (86.88e6, "profiles/temporal_kernel_dram_alu_captures.md", "8b09bac81d9f47a3"),
-    ("excitable", "temporal", 16, 16384): (152.15e6, "profiles/temporal_kernel_dram_alu_captures.md", "01d9d66fd15fd82b"),
-    ("cyclic", "temporal", 8, 32768): (1293.26e6, "profiles/temporal_kernel_dram_alu_captures.md", "de7c1cb4beff04ff"),
-    ("fluid", "temporal", 16, 32768): (1025.61e6, "profiles/temporal_kernel_dram_alu_captures.md", "7f66e007783f5d50"),
+    ("wire", "temporal", 16, 16384): (86.81e6, "profiles/temporal_kernel_dram_alu_captures.md", "99f07bc533075f2b"),
+    ("excitable", "temporal", 16, 16384): (152.60e6, "profiles/temporal_kernel_dram_alu_captures.md", "c912b66d798e9644"),
+    ("cyclic", "temporal", 8, 32768): (1293.47e6, "profiles/temporal_kernel_dram_alu_captures.md", "aed4cd45da7b7fcf"),
+    ("fluid", "temporal", 16, 32768): (1025.98e6, "profiles/temporal_kernel_dram_alu_captures.md", "81fa5ee2a3685590"),
 }
 
 # ALU-pipe warp instructions (smsp__inst_executed_pipe_alu.sum) per launch of a
@@ -81,10 +81,10 @@ MEASURED_TRAFFIC = {
 # Each configuration is timed live and set against the ALU pipe's measured rate
 # (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
-    ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "8b09bac81d9f47a3"),
-    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (71637912, "profiles/temporal_kernel_dram_alu_captures.md", "01d9d66fd15fd82b"),
-    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "de7c1cb4beff04ff"),
-    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "7f66e007783f5d50"),
+    ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "99f07bc533075f2b"),
+    ("excitable", 1, 32, 16, 0, 3, 1, 16384): (71637912, "profiles/temporal_kernel_dram_alu_captures.md", "c912b66d798e9644"),
+    ("cyclic", 0, 64, 8, 160, 2, 1, 32768): (813584240, "profiles/temporal_kernel_dram_alu_captures.md", "aed4cd45da7b7fcf"),
+    ("fluid", 0, 64, 16, 0, 3, 1, 32768): (326666480, "profiles/temporal_kernel_dram_alu_captures.md", "81fa5ee2a3685590"),
 }
 
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
