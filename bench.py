@@ -486,51 +486,59 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
     d2h = h2d
     L = lib.load()
 
-    # Copies run on two copy streams so that one automaton's upload and the
-    # other's download overlap the compute; events order each buffer's reuse:
-    # an upload waits for the previous download of the same automaton, the
-    # compute for its upload, the download for its compute.
+    # Copies run on two copy streams, and each automaton has two device plane
+    # sets used by alternate steps: a step's upload overlaps the previous
+    # step's compute, and its download the next step's.  Events order each
+    # set's reuse: an upload waits for the download from the same set two steps
+    # earlier, the compute for its upload, the download for its compute.
     cs_in, cs_out = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
-    in_ready = {a: torch.cuda.Event() for a in AUTOMATA}
-    computed = {a: torch.cuda.Event() for a in AUTOMATA}
-    out_done = {a: torch.cuda.Event() for a in AUTOMATA}
+    sets = {a: [(g["a"], g["b"]), (DevicePlanes(g["nb"], X, Y, dev), DevicePlanes(g["nb"], X, Y, dev))]
+            for a, g in grids.items()}
+    in_ready = {a: [torch.cuda.Event(), torch.cuda.Event()] for a in AUTOMATA}
+    computed = {a: [torch.cuda.Event(), torch.cuda.Event()] for a in AUTOMATA}
+    out_done = {a: [torch.cuda.Event(), torch.cuda.Event()] for a in AUTOMATA}
     start_ev = torch.cuda.Event()
 
-    def e2e_step(t0):
+    def e2e_step(i, t0):
+        par = i & 1
         for a, g in grids.items():
             nb, pb_ = g["nb"], g["init"].plane_bytes
+            pa, _ = sets[a][par]
             cs_in.wait_event(start_ev)
-            cs_in.wait_event(out_done[a])
-            lib.check(L.cellato_planes_upload(nb, lib.ptr_array(g["a"].ptrs),
+            cs_in.wait_event(out_done[a][par])
+            lib.check(L.cellato_planes_upload(nb, lib.ptr_array(pa.ptrs),
                                               lib.ptr_array([t.data_ptr() for t in host_in[a]]), pb_,
                                               cs_in.cuda_stream))
-            in_ready[a].record(cs_in)
+            in_ready[a][par].record(cs_in)
         for a, g in grids.items():
             nb, pb_ = g["nb"], g["init"].plane_bytes
+            pa, pb = sets[a][par]
             st = stream if args.sequential else comp[a]
-            st.wait_event(in_ready[a])
-            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, g["W"], g["a"].ptrs, g["b"].ptrs, X, Y, t0,
+            st.wait_event(in_ready[a][par])
+            in_b = autotune.run(g["choice"], g["rule"], LAYOUT, g["W"], pa.ptrs, pb.ptrs, X, Y, t0,
                                 args.ca_steps, st.cuda_stream)
-            computed[a].record(st)
-            res = g["b"] if in_b else g["a"]
-            cs_out.wait_event(computed[a])
+            computed[a][par].record(st)
+            res = pb if in_b else pa
+            cs_out.wait_event(computed[a][par])
             lib.check(L.cellato_planes_download(nb, lib.ptr_array([t.data_ptr() for t in host_out[a]]),
                                                 lib.ptr_array(res.ptrs), pb_, cs_out.cuda_stream))
-            out_done[a].record(cs_out)
+            out_done[a][par].record(cs_out)
 
     for a in AUTOMATA:
-        out_done[a].record(cs_out)
+        for par in (0, 1):
+            out_done[a][par].record(cs_out)
     start_ev.record(stream)
-    e2e_step(0)
+    e2e_step(0, 0)
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     start_ev.record(stream)
-    for _ in range(args.steps):
-        e2e_step(0)
+    for i in range(args.steps):
+        e2e_step(i, 0)
     for a in AUTOMATA:
-        stream.wait_event(out_done[a])   # the timed region ends after the last download
+        for par in (0, 1):
+            stream.wait_event(out_done[a][par])   # the timed region ends after the last download
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -545,6 +553,7 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
         res = g["b"] if in_b else g["a"]
         torch.cuda.synchronize()
         e2e_ok &= all(torch.equal(res.view(p).cpu(), host_out[a][p]) for p in range(g["nb"]))
+    del sets
 
     peaks = measured_peaks()
     # ---- the best single-step kernel of each automaton against the HBM roofline
@@ -660,8 +669,9 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
         "per_automaton_gcups": {a: round(v, 1) for a, v in per_gcups.items()},
         "e2e": {"value": round(e2e_value, 1), "unit": "GCUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "result_checked": bool(e2e_ok),
-                "note": "pinned host planes through the C ABI; uploads and downloads on two copy streams, "
-                        "overlapping the other automaton's compute"},
+                "note": "pinned host planes through the C ABI; uploads and downloads on two copy streams, two "
+                        "device plane sets per automaton used by alternate steps, so a step's copies overlap the "
+                        "neighbouring steps' compute"},
         "gpu_launches": n_launch,
         "roofline": roof,
         "single_step_roofline": {"peak_gbs": peaks["hbm_gbs"], "peak_source": peaks["source"], **single},
