@@ -36,7 +36,7 @@ EXPORTED = [
     "cellato_server_create", "cellato_server_submit_random", "cellato_server_submit_planes",
     "cellato_server_iterate", "cellato_server_poll", "cellato_server_planes", "cellato_server_release",
     "cellato_server_stats_get", "cellato_server_destroy", "cellato_server_submit_resume",
-    "cellato_server_snapshot", "cellato_server_cancel", "cellato_lop3_rate",
+    "cellato_server_snapshot", "cellato_server_cancel",
 ]
 
 
@@ -123,7 +123,6 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     ll = ctypes.c_longlong
     lib.cellato_checksum.argtypes = [i, i, i, _PP, i, i, _vp, _vp]
     lib.cellato_diff_cells.argtypes = [i, _PP, _PP, ctypes.c_size_t, _vp, _vp]
-    lib.cellato_lop3_rate.argtypes = [ctypes.POINTER(ctypes.c_double), _vp]
     lib.cellato_bit_array_bytes.argtypes = [i, i, i, i]
     lib.cellato_bit_array_bytes.restype = ctypes.c_size_t
     lib.cellato_bit_array_to_planes.argtypes = [i, i, _vp, i, i, i, i, _PP, _vp]
@@ -284,14 +283,6 @@ def diff_cells(nb: int, planes_a, planes_b, plane_bytes: int, count_ptr: int, st
     """Number of differing cells between two grids of the same layout, into one
     uint64 of device memory at count_ptr."""
     check(load().cellato_diff_cells(nb, ptr_array(planes_a), ptr_array(planes_b), plane_bytes, count_ptr, stream))
-
-
-def lop3_rate(stream: int = 0) -> float:
-    """Measured LOP3 lane-operations per second of the current device (the ALU
-    pipe's peak for the temporal kernels' compute roofline)."""
-    v = ctypes.c_double(0.0)
-    check(load().cellato_lop3_rate(ctypes.byref(v), stream))
-    return v.value
 
 
 def bit_array_to_planes(nb: int, array_word_bits: int, array_ptr: int, X: int, Y: int, layout: int, word_bits: int,

@@ -79,7 +79,7 @@ MEASURED_TRAFFIC = {
 # (summary in profiles/); keyed by (rule, layout, word size, k, tile_rows, row
 # loop, words per lane, size), tile_rows 0 being the library's default height.
 # Each configuration is timed live and set against the ALU pipe's measured rate
-# (cellato_lop3_rate) for the compute roofline.  Source hashes as above.
+# (lop3_rate) for the compute roofline.  Source hashes as above.
 MEASURED_ALU = {
     ("wire", 1, 32, 16, 0, 3, 1, 16384): (111137328, "profiles/temporal_kernel_dram_alu_captures.md", "99f07bc533075f2b"),
     ("excitable", 1, 32, 16, 0, 3, 1, 16384): (71637912, "profiles/temporal_kernel_dram_alu_captures.md", "c912b66d798e9644"),
@@ -90,6 +90,23 @@ MEASURED_ALU = {
 AUTOMATON_DIRS = {"game-of-life": "game_of_life", "forest-fire": "fire", "wire": "wire", "excitable": "excitable",
                   "brian": "brian", "maze": "maze", "cyclic": "cyclic", "fluid": "fluid", "critters": "critters",
                   "traffic": "traffic"}
+
+
+LOP3_RATE_LIB = os.path.join(ROOT, "_build", "liblop3_rate.so")
+
+
+def lop3_rate(stream: int = 0) -> float:
+    """Measured LOP3 lane-operations per second of the current device, the ALU
+    pipe's peak for the temporal kernels' compute roofline (lop3_rate.cu, built
+    by __graft_entry__.build())."""
+    import ctypes
+    so = ctypes.CDLL(LOP3_RATE_LIB)
+    so.lop3_rate.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    v = ctypes.c_double(0.0)
+    rc = so.lop3_rate(ctypes.byref(v), stream)
+    if rc != 0:
+        raise RuntimeError(f"lop3_rate failed with CUDA error {rc}")
+    return v.value
 
 
 def kernel_source_hash(rule: str) -> str:
@@ -591,8 +608,8 @@ def our_arm(args, rank: int, world: int, cpu_baseline: bool = True):
     # launch (ncu count of the configuration) over the live launch time, against
     # the ALU pipe's measured LOP3 rate on this device
     alu = {"bound": "alu", "unit": "Gop/s (32-bit lane operations)",
-           "peak": round(lib.lop3_rate(sp) / 1e9, 1),
-           "peak_source": "measured live: cellato_lop3_rate (independent lop3.b32 chains, full occupancy)",
+           "peak": round(lop3_rate(sp) / 1e9, 1),
+           "peak_source": "measured live: lop3_rate.cu (independent lop3.b32 chains, full occupancy)",
            "kernels": {}}
     # one capture per automaton: the timed configuration's when there is one
     picked = {}

@@ -323,14 +323,6 @@ int cellato_fill_random(int layout, int word_bits, int nb, void* const* planes, 
                         unsigned long long seed, const uint32_t* thresholds, int n_thresholds,
                         cellato_stream_t stream);
 
-/* Measured peak of the ALU (integer/logic) pipe: LOP3 lane-operations per
- * second on the current device, the best of three launches of a kernel that
- * keeps every SM at full occupancy with independent lop3.b32 chains.  It is
- * the compute roofline's denominator for the temporal kernels, whose ALU
- * instructions per launch come from an ncu count.  Synchronises `stream`
- * (allocates and frees a small sink buffer).  No counterpart in the reference. */
-int cellato_lop3_rate(double* lane_ops_per_second, cellato_stream_t stream);
-
 /* ---- simulation server: continuous batching of many requests ------------
  * No counterpart in the reference (one grid per CLI run).  A request is one
  * grid of one automaton advanced `steps` steps from step 0; the server keeps

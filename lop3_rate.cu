@@ -1,5 +1,7 @@
 // Measured peak of the ALU pipe for the compute roofline of the temporal
-// kernels (C ABI cellato_lop3_rate).  No counterpart in the reference.
+// kernels: measurement infrastructure of bench.py and profile_case.py, built
+// into its own library (_build/liblop3_rate.so) by __graft_entry__.build(),
+// not part of the B200 library or its C ABI.  No counterpart in the reference.
 //
 // The temporal kernels run k steps per launch out of shared memory, so HBM
 // bounds them only at small k; above that, they are bound by the integer/logic
@@ -14,11 +16,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-
-#include "capi_internal.hpp"
-#include "cellato_b200.h"
-
-using namespace cellato::b200::capi;
 
 namespace {
 
@@ -60,13 +57,16 @@ __global__ void __launch_bounds__(RATE_THREADS) lop3_rate_kernel(int trips, uint
 
 extern "C" {
 
-int cellato_lop3_rate(double* lane_ops_per_second, cellato_stream_t stream) {
-    if (!lane_ops_per_second) return fail(CELLATO_EINVAL, "lane_ops_per_second must not be NULL");
+// Best LOP3 lane-operations per second of three timed launches on `stream`
+// (a cudaStream_t) of the current device; synchronises the stream.  Returns a
+// cudaError_t (0 on success).
+int lop3_rate(double* lane_ops_per_second, void* stream) {
+    if (!lane_ops_per_second) return (int)cudaErrorInvalidValue;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return cuda_fail(e, "device query");
+    if (e != cudaSuccess) return (int)e;
     const int ctas = sms * RATE_CTAS_PER_SM;
     const size_t threads = (size_t)ctas * RATE_THREADS;
     uint32_t* sink = nullptr;
@@ -98,9 +98,9 @@ int cellato_lop3_rate(double* lane_ops_per_second, cellato_stream_t stream) {
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (sink) cudaFree(sink);
-    if (e != cudaSuccess) return cuda_fail(e, "LOP3 rate kernel");
+    if (e != cudaSuccess) return (int)e;
     *lane_ops_per_second = best;
-    return CELLATO_OK;
+    return 0;
 }
 
 }  // extern "C"

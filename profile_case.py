@@ -31,7 +31,7 @@ def main() -> None:
     ap.add_argument("--mode", default="temporal", choices=["simple", "temporal", "ops", "lop3", "batch"],
                     help="ops: the whole-grid operations (checksum, diff, random fill, packing, bit_array "
                          "conversion), each run --launches times; lop3: the ALU-pipe rate kernel "
-                         "(cellato_lop3_rate: one warm-up and three timed launches)")
+                         "(lop3_rate.cu: one warm-up and three timed launches)")
     ap.add_argument("--k", type=int, default=8)
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--loop", type=int, default=0, help="temporal row loop (cellato_tune.row_loop)")
@@ -46,7 +46,8 @@ def main() -> None:
 
     r = lib.rule_id(a.rule)
     if a.mode == "lop3":
-        print(json.dumps({"lop3_lane_ops_per_s": lib.lop3_rate()}))
+        from bench import lop3_rate
+        print(json.dumps({"lop3_lane_ops_per_s": lop3_rate()}))
         return
     if a.mode == "ops":
         return ops(a, r)
