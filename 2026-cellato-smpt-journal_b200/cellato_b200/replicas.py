@@ -54,6 +54,16 @@ def max_over_ranks(x: float) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(x: float) -> float:
+    """The sum over the ranks (units of work that differ per rank)."""
+    import torch
+    if not torch.distributed.is_initialized():
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=_device())
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+    return float(t.item())
+
+
 def job_rate(units_per_rank: float, world: int, max_ms: float) -> float:
     """Whole-job throughput: the units all ranks processed over the slowest
     rank's time, per second."""

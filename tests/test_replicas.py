@@ -28,12 +28,13 @@ def _worker(rank, world, port, queue):
     r, w = replicas.init(timeout_s=60, backend="gloo")
     replicas.barrier()
     slowest = replicas.max_over_ranks(10.0 + 5.0 * r)     # ms of this rank's timed region
-    queue.put((r, w, slowest, replicas.job_rate(2e9, w, slowest)))
+    total = replicas.sum_over_ranks(1000.0 + r)            # work units that differ per rank
+    queue.put((r, w, slowest, replicas.job_rate(2e9, w, slowest), total))
     replicas.barrier()
     replicas.shutdown()
 
 
-def test_two_gloo_ranks_agree_on_the_slowest_time():
+def test_two_gloo_ranks_agree_on_the_slowest_time_and_the_sum():
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -48,6 +49,7 @@ def test_two_gloo_ranks_agree_on_the_slowest_time():
     assert [o[0] for o in out] == [0, 1] and all(o[1] == 2 for o in out)
     assert all(o[2] == 15.0 for o in out)              # both ranks see the max
     assert all(abs(o[3] - 2 * 2e9 / 15e-3) < 1 for o in out)
+    assert all(o[4] == 2001.0 for o in out)            # both ranks see the sum
 
 
 def test_bench_reference_arm_under_torchrun_two_ranks():
