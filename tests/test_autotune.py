@@ -24,6 +24,20 @@ def test_legal_candidates_filter():
     assert autotune.legal_candidates([("temporal", 24, 48, 1, 1)], planes=1, band_rows=1) == []
 
 
+def test_candidate_sets_cover_widths_and_row_loops():
+    """TMA widths 1, 2, 4 as single-step candidates, four words per lane only
+    for one-plane rules; the three row loops among the temporal candidates."""
+    tma = [c for c in autotune.SINGLE_STEP_CANDIDATES if c[0] == "simple_tma"]
+    assert {c[4] for c in tma if len(c) > 4} == {1, 2, 4}
+    widths = lambda planes: sorted({c["width"] for c in autotune.legal_candidates(tma, planes=planes)})
+    assert widths(1) == [0, 1, 2, 4] and widths(2) == [0, 1, 2] and widths(5) == [0, 1]
+    loops = {c[3] for c in autotune.DEFAULT_CANDIDATES if c[0] == "temporal" and len(c) > 3}
+    assert loops == {1, 2, 3}
+    # two steps per sweep at k = 1 would be the hoisted loop: not a candidate
+    assert not [c for c in autotune.DEFAULT_CANDIDATES if c[0] == "temporal" and c[1] == 1 and len(c) > 3
+                and c[3] == 3]
+
+
 def test_pick_takes_the_earliest_within_the_tie_band():
     a, b, c = {"k": 1}, {"k": 8}, {"k": 16}
     assert autotune.pick([(a, 1.00), (b, 0.99), (c, 0.90)])["k"] == 16
